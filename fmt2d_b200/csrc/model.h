@@ -1,0 +1,94 @@
+// Host-side model geometry for the device solver.
+//
+// The propagation grid, the five interfaces and the six regions follow the
+// reference's model build (propagate2d.f90:1335-1979, invert2d_main.f90:139-
+// 500) so that region node numbering, cut cells and the fully-regular mask
+// are bit-exact.  The device layout is this library's own: every region is a
+// dense row band of the grid ("bbox") padded to a pitch, followed by two rows
+// holding the region's top and bottom interface nodes.  A "slot" indexes that
+// layout; all per-node device arrays of a region are slot-indexed.
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <string>
+
+namespace fmt2d {
+
+constexpr double kHugeTime = 1.0e20;
+constexpr int kTileW = 32;   // tile width (columns) of the eikonal sweeps
+constexpr int kTileH = 32;   // tile height (rows)
+
+// Per-slot static code (uint32):
+//   bit 0      node belongs to the region
+//   bit 1      updatable (interface nodes in an unregistered cut cell are not)
+//   bit 2      fully regular (4 regular quadrants)
+//   bit 3      interface node (slot in one of the two interface rows)
+//   bits 4-7   cell exists, cells c=0..3 = (ix,iz),(ix,iz-1),(ix-1,iz),(ix-1,iz-1)
+//   bits 8-11  cell is cut by the region's own top/bottom interface
+//   bits 12-15 that cut cell carries a top-interface inode
+//   bits 16-19 that cut cell carries a bottom-interface inode
+// Interface slots: bits 8 (own cut cell irregular), 12/16 (top/bottom inodes
+// present in that cell); the cell's top row is in Region::izc_top/izc_bot.
+enum : uint32_t {
+  kInRegion = 1u << 0,
+  kUpdatable = 1u << 1,
+  kFullyRegular = 1u << 2,
+  kIfaceNode = 1u << 3,
+};
+inline uint32_t cell_exists_bit(int c) { return 1u << (4 + c); }
+inline uint32_t cell_irr_bit(int c) { return 1u << (8 + c); }
+inline uint32_t cell_top_bit(int c) { return 1u << (12 + c); }
+inline uint32_t cell_bot_bit(int c) { return 1u << (16 + c); }
+
+struct Interface {
+  std::vector<double> z;          // node depth (node ix sits on grid column ix)
+  std::vector<double> nrm_x, nrm_z;
+  std::vector<double> vel_top, vel_bot;
+  std::vector<int> izc;           // cut cell row (0-based), -1 if none
+  std::vector<uint8_t> inode_ok;  // node lies inside its cut cell's rows
+};
+
+struct Region {
+  int id = 0, itop = 0, ibot = 0;           // 1-based interface ids
+  int ngnode = 0, nnode = 0;
+  int z_lo = 0, z_hi = -1, H = 0, pitch = 0; // bbox rows (0-based), slot pitch
+  int tiles_x = 0, tiles_y = 0;
+  std::vector<int> r0, r1;                   // per column first/last row (r1<r0 empty)
+  std::vector<int> col_base;                 // node id of the column's first node - 1
+  std::vector<uint32_t> code;                // per slot
+  std::vector<float> vel;                    // per slot
+  std::vector<float> iface_dz;               // per interface slot (2*pitch): z - z(izc)
+  std::vector<int> izc_top, izc_bot;         // cut-cell rows of the two interfaces
+  std::vector<int> slot_of_node;             // region node id (0-based) -> slot
+  size_t nslots() const { return (size_t)(H + 2) * pitch; }
+  int slot_grid(int ix, int iz) const { return (iz - z_lo) * pitch + ix; }
+  int slot_top(int ix) const { return H * pitch + ix; }
+  int slot_bot(int ix) const { return (H + 1) * pitch + ix; }
+};
+
+struct Model {
+  int nx = 0, nz = 0;
+  double dx = 0, x0 = 0, tolerance = 0, vwater = 1.5;
+  std::vector<double> xpos;                 // smesh node x (for the velocity grid)
+  std::vector<double> vel;                  // pgrid velocity, ix fastest
+  std::vector<uint8_t> cell_cut;            // per cell: bit k = interface k cuts it
+  std::vector<int> node_region, rnode_id;   // last region claiming a grid node
+  std::vector<uint8_t> fully_regular;
+  Interface ifc[6];                         // 1..5
+  Region reg[7];                            // 1..6
+  // interface node id tables as left by the reference's region definitions
+  std::vector<int> rright[6], rleft[6];
+  // inversion numbering (iz outer, ix inner over nodes at or below the seafloor)
+  std::vector<int> inv_idx;
+  int n_vel_parms = 0, n_inv_parms = 0, iface_inv = 0;
+  size_t g(int ix, int iz) const { return (size_t)iz * nx + ix; }
+};
+
+// Builds the model from smesh-level inputs (read_smesh outputs plus the two
+// interface files), resampling like invert2d_main.f90:279-340.
+// Returns an empty string on success or an error message.
+std::string build_model(Model& m, int nx, int nzs, const double* xpos, const double* topo,
+                        const double* zrel, const double* vel, double vwater,
+                        const double* sed_z, const double* moho_z, int iface_inv);
+
+}  // namespace fmt2d

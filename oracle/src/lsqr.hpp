@@ -1,0 +1,35 @@
+// Oracle LSQR interfaces.  TEST INFRASTRUCTURE ONLY (see oracle.hpp).
+#pragma once
+
+namespace orc {
+
+struct LsqrGeom {
+  int nx = 0, nz = 0;
+  const int* inv_idx = nullptr;   // nx*nz, ix fastest, 1-based ids, 0 inactive
+  int iface_start = 0, iface_nx = 0;
+};
+
+struct LsqrInput {
+  int ndata = 0, nparm = 0, n_vel_parms = 0, max_iter = 0;
+  const int* gindx = nullptr;     // 1-based column ids
+  const double* gval = nullptr;
+  const int* row_ptr = nullptr;   // 1-based, ndata+1 entries
+  const double* residual = nullptr;
+  const double* gtg_diag = nullptr;
+  const double* dm_sum = nullptr;
+  double eps_min = 0, wdv = 0, wdv_iface = 0, w_smooth = 0, w_smooth_iface = 0;
+};
+
+struct LsqrResult {
+  int iters = 0;
+  double rnorm = 0, bnorm = 0, test2 = 0;
+};
+
+void sparse_Ax(int ndata, int nparm, const int* gindx, const double* gval, const int* row_ptr,
+               const double* x, double* y);
+void sparse_ATx(int ndata, int nparm, const int* gindx, const double* gval, const int* row_ptr,
+                const double* y, double* x);
+void laplacian(const LsqrGeom& G, int nparm, const double* vin, double* vout);
+LsqrResult run_lsqr_laplacian(const LsqrGeom& G, const LsqrInput& in, double* dm);
+
+}  // namespace orc
