@@ -1,0 +1,69 @@
+"""ctypes binding of the C ABI in include/fmt2d_gpu.h.
+
+The shared library is built in-tree (fmt2d_b200/_lib/libfmt2d_b200.so) by
+`fmt2d_b200.build.build()`.  There is no fallback: if the library is missing
+or fails to load, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libfmt2d_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "fmt2d_gpu.h")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("nzs", C.c_int), ("xpos", C.c_void_p), ("topo", C.c_void_p),
+                ("zrel", C.c_void_p), ("vel", C.c_void_p), ("vwater", C.c_double),
+                ("sed_z", C.c_void_p), ("moho_z", C.c_void_p), ("iface_inv", C.c_int)]
+
+
+class Fmt2dError(RuntimeError):
+    pass
+
+
+def header_symbols() -> list[str]:
+    """Every function the C header declares."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"FMT2D_API\s+int\s+(fmt2d_\w+)\s*\(", txt)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise Fmt2dError(f"native library not built: {LIB_PATH} (run fmt2d_b200.build.build())")
+    L = C.CDLL(LIB_PATH)
+    V = C.c_void_p
+    P = C.POINTER
+    L.fmt2d_ctx_create.argtypes = [P(V), C.c_int]
+    L.fmt2d_ctx_destroy.argtypes = [V]
+    L.fmt2d_last_error.argtypes = [V, C.c_char_p, C.c_int]
+    L.fmt2d_upload_model.argtypes = [V, P(ModelDesc)]
+    L.fmt2d_model_info.argtypes = [V, P(C.c_int), P(C.c_int), P(C.c_double), P(C.c_double)]
+    L.fmt2d_region_nodes.argtypes = [V, C.c_int, P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fmt2d_inv_index.argtypes = [V, C.c_void_p, P(C.c_int), P(C.c_int)]
+    L.fmt2d_forward.argtypes = [V, _dp, C.c_int, C.c_int]
+    L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fmt2d_forward_stats.argtypes = [V, P(C.c_int), P(C.c_int), P(C.c_int),
+                                      P(C.c_longlong), P(C.c_double)]
+    for name in header_symbols():
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

@@ -1,0 +1,124 @@
+"""Python host interface of the B200 forward-and-sensitivity path.
+
+Mirrors the reference's operator interface for the path: a model built from
+read_smesh-level arrays, `forward` solving the time fields of the enabled
+phases for every OBS source (run_forward2d's stage loop,
+src/inversion2d.f90:4184-4476), and field access in the reference's region
+node order.  All work goes through the C ABI of include/fmt2d_gpu.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .synth import SmeshModel
+
+PHASES = {"Pg": 1, "PsedP": 2, "PmP": 3, "Pg_ss": 4, "Pg_ss2": 5}
+TF_REGION = {1: 5, 2: 2, 3: 2, 4: 6, 5: 6, 6: 1, 7: 1, 8: 1, 9: 1, 10: 1, 11: 5, 12: 1}
+PHASE_FIELDS = {1: (1,), 2: (2, 3), 3: (4, 5), 4: (1, 6, 7, 8), 5: (9, 10, 11, 12)}
+
+
+def phase_mask(phases) -> int:
+    m = 0
+    for p in phases:
+        m |= 1 << ((PHASES[p] if isinstance(p, str) else int(p)) - 1)
+    return m
+
+
+def fields_of(mask: int) -> list[int]:
+    out = set()
+    for p in range(1, 6):
+        if mask & (1 << (p - 1)):
+            out.update(PHASE_FIELDS[p])
+    return sorted(out)
+
+
+class Fmt2d:
+    """One context (device buffers + stream).  device=-1 gives a host-only
+    context for the model tables."""
+
+    def __init__(self, device: int = 0):
+        self.L = N.lib()
+        h = C.c_void_p()
+        rc = self.L.fmt2d_ctx_create(C.byref(h), int(device))
+        if rc != 0:
+            raise N.Fmt2dError(f"fmt2d_ctx_create(device={device}) failed with code {rc}")
+        self.h = h
+        self.device = device
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fmt2d_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.L.fmt2d_last_error(self.h, buf, 512)
+            raise N.Fmt2dError(f"{what} failed ({rc}): {buf.value.decode()}")
+
+    def upload(self, m: SmeshModel, iface_inv: int = 4):
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        keep = [f(m.xpos), f(m.topo), f(m.zrel), f(m.vel), f(m.sed_z), f(m.moho_z)]
+        d = N.ModelDesc(m.nx, m.zrel.size, N.ptr(keep[0]), N.ptr(keep[1]), N.ptr(keep[2]),
+                        N.ptr(keep[3]), float(m.vwater), N.ptr(keep[4]), N.ptr(keep[5]),
+                        int(iface_inv))
+        self._check(self.L.fmt2d_upload_model(self.h, C.byref(d)), "fmt2d_upload_model")
+        nx, nz, dx, x0 = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+        self._check(self.L.fmt2d_model_info(self.h, C.byref(nx), C.byref(nz), C.byref(dx),
+                                            C.byref(x0)), "fmt2d_model_info")
+        self.nx, self.nz, self.dx, self.x0 = nx.value, nz.value, dx.value, x0.value
+        self.model = m
+        return self
+
+    def region_nodes(self, r: int):
+        n = C.c_int()
+        self._check(self.L.fmt2d_region_nodes(self.h, r, C.byref(n), None, None, None),
+                    "fmt2d_region_nodes")
+        i1, i2, i3 = (np.zeros(n.value, np.int32) for _ in range(3))
+        self._check(self.L.fmt2d_region_nodes(self.h, r, C.byref(n), N.ptr(i1), N.ptr(i2),
+                                              N.ptr(i3)), "fmt2d_region_nodes")
+        return i1, i2, i3
+
+    def region_nnode(self, r: int) -> int:
+        n = C.c_int()
+        self._check(self.L.fmt2d_region_nodes(self.h, r, C.byref(n), None, None, None),
+                    "fmt2d_region_nodes")
+        return n.value
+
+    def inv_index(self):
+        out = np.zeros(self.nx * self.nz, np.int32)
+        nvp, npar = C.c_int(), C.c_int()
+        self._check(self.L.fmt2d_inv_index(self.h, N.ptr(out), C.byref(nvp), C.byref(npar)),
+                    "fmt2d_inv_index")
+        return out.reshape(self.nz, self.nx), nvp.value, npar.value
+
+    def forward(self, src_x, phases=(1, 2, 3, 4, 5)):
+        src_x = np.ascontiguousarray(src_x, dtype=np.float64)
+        self.mask = phase_mask(phases)
+        self._check(self.L.fmt2d_forward(self.h, src_x, src_x.size, self.mask), "fmt2d_forward")
+        self.nsrc = src_x.size
+        return self
+
+    def field(self, src: int, tf: int):
+        n = self.region_nnode(TF_REGION[tf])
+        T, gx, gz = np.zeros(n), np.zeros(n), np.zeros(n)
+        self._check(self.L.fmt2d_get_field(self.h, src, tf, N.ptr(T), N.ptr(gx), N.ptr(gz)),
+                    "fmt2d_get_field")
+        return T, gx, gz
+
+    def stats(self):
+        a, b, c, v, ms = C.c_int(), C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        self._check(self.L.fmt2d_forward_stats(self.h, C.byref(a), C.byref(b), C.byref(c),
+                                               C.byref(v), C.byref(ms)), "fmt2d_forward_stats")
+        return dict(rounds=a.value, batches=b.value, final_passes=c.value, tile_visits=v.value,
+                    round_ms=round(ms.value, 3))

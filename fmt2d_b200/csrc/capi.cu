@@ -1,0 +1,157 @@
+// C ABI entry points (include/fmt2d_gpu.h).
+#include "../../include/fmt2d_gpu.h"
+#include "engine.h"
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+struct fmt2d_ctx {
+  std::unique_ptr<fmt2d::Engine> eng;   // null for a host-only context
+  fmt2d::Model model;
+  std::string err;
+  bool has_model = false;
+  bool need_gpu(int& code) {
+    if (eng) return true;
+    err = "host-only context (device -1): no GPU work possible";
+    code = FMT2D_ERR_STATE;
+    return false;
+  }
+  int fail(int code, const std::string& msg) {
+    err = msg;
+    return code;
+  }
+};
+
+extern "C" {
+
+int fmt2d_ctx_create(fmt2d_ctx** out, int device) {
+  if (!out) return FMT2D_ERR_ARG;
+  *out = nullptr;
+  if (device == -1) {  // host-only: model build and tables, no device work
+    fmt2d_ctx* c = new (std::nothrow) fmt2d_ctx();
+    if (!c) return FMT2D_ERR_ARG;
+    *out = c;
+    return FMT2D_OK;
+  }
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return FMT2D_ERR_CUDA;
+  fmt2d_ctx* c = new (std::nothrow) fmt2d_ctx();
+  if (!c) return FMT2D_ERR_ARG;
+  c->eng.reset(new fmt2d::Engine(device));
+  if (cudaGetLastError() != cudaSuccess) {
+    delete c;
+    return FMT2D_ERR_CUDA;
+  }
+  *out = c;
+  return FMT2D_OK;
+}
+
+int fmt2d_ctx_destroy(fmt2d_ctx* ctx) {
+  delete ctx;
+  return FMT2D_OK;
+}
+
+int fmt2d_last_error(fmt2d_ctx* ctx, char* buf, int len) {
+  if (!ctx || !buf || len <= 0) return FMT2D_ERR_ARG;
+  std::strncpy(buf, ctx->err.c_str(), (size_t)len - 1);
+  buf[len - 1] = '\0';
+  return FMT2D_OK;
+}
+
+int fmt2d_upload_model(fmt2d_ctx* ctx, const fmt2d_model_desc* d) {
+  if (!ctx || !d) return FMT2D_ERR_ARG;
+  if (!d->xpos || !d->topo || !d->zrel || !d->vel || !d->sed_z || !d->moho_z)
+    return ctx->fail(FMT2D_ERR_ARG, "null model array");
+  if (d->nx < 3 || d->nzs < 2) return ctx->fail(FMT2D_ERR_ARG, "model too small");
+  ctx->has_model = false;
+  std::string e = fmt2d::build_model(ctx->model, d->nx, d->nzs, d->xpos, d->topo, d->zrel,
+                                     d->vel, d->vwater, d->sed_z, d->moho_z, d->iface_inv);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_MODEL, e);
+  if (ctx->eng) {
+    e = ctx->eng->upload(ctx->model);
+    if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  }
+  ctx->has_model = true;
+  return FMT2D_OK;
+}
+
+int fmt2d_model_info(fmt2d_ctx* ctx, int* nx, int* nz, double* dx, double* x0) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const fmt2d::Model& m = ctx->model;
+  if (nx) *nx = m.nx;
+  if (nz) *nz = m.nz;
+  if (dx) *dx = m.dx;
+  if (x0) *x0 = m.x0;
+  return FMT2D_OK;
+}
+
+int fmt2d_region_nodes(fmt2d_ctx* ctx, int region, int* nnode, int* i1, int* i2, int* i3) {
+  if (!ctx || region < 1 || region > 6) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const fmt2d::Model& m = ctx->model;
+  const fmt2d::Region& r = m.reg[region];
+  if (nnode) *nnode = r.nnode;
+  if (!i1 && !i2 && !i3) return FMT2D_OK;
+  for (int ix = 0; ix < m.nx; ++ix)
+    for (int iz = r.r0[ix]; iz <= r.r1[ix]; ++iz) {
+      const int id = r.col_base[ix] + (iz - r.r0[ix]);
+      if (i1) i1[id] = ix + 1;
+      if (i2) i2[id] = iz + 1;
+      if (i3) i3[id] = 0;
+    }
+  for (int k = 0; k < m.nx; ++k) {
+    const int a = r.ngnode + k, b = r.ngnode + m.nx + k;
+    if (i1) { i1[a] = 0; i1[b] = 0; }
+    if (i2) { i2[a] = r.itop; i2[b] = r.ibot; }
+    if (i3) { i3[a] = k + 1; i3[b] = k + 1; }
+  }
+  return FMT2D_OK;
+}
+
+int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* nvp, int* npar) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const fmt2d::Model& m = ctx->model;
+  if (inv_idx) std::memcpy(inv_idx, m.inv_idx.data(), m.inv_idx.size() * sizeof(int));
+  if (nvp) *nvp = m.n_vel_parms;
+  if (npar) *npar = m.n_inv_parms;
+  return FMT2D_OK;
+}
+
+int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask) {
+  if (!ctx || !src_x || nsrc <= 0 || (phase_mask & ~31) || !phase_mask) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const std::string e = ctx->eng->forward(src_x, nsrc, phase_mask);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  return FMT2D_OK;
+}
+
+int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, double* gz) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const std::string e = ctx->eng->get_field(src, tf, T, gx, gz);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  return FMT2D_OK;
+}
+
+int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* finals,
+                        long long* visits, double* round_ms) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const fmt2d::SolveStats& s = ctx->eng->stats();
+  if (rounds) *rounds = s.rounds;
+  if (batches) *batches = s.batches;
+  if (finals) *finals = s.final_passes;
+  if (visits) *visits = s.tile_visits;
+  if (round_ms) *round_ms = s.round_ms;
+  return FMT2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,321 @@
+// Host-side model build for the device solver (see model.h for the layout).
+#include "model.h"
+#include <algorithm>
+#include <cmath>
+
+namespace fmt2d {
+
+namespace {
+
+// Depth of an interface at horizontal position px: linear between nodes,
+// clamped to the end nodes (propagate2d.f90:1623-1645 and rays2d.f90:1222).
+double iface_z_at(const Model& m, const std::vector<double>& xs, const std::vector<double>& zs,
+                  double px) {
+  const int n = (int)zs.size();
+  if (n < 2) return zs[0];
+  const int k = (int)std::floor((px - xs[0]) / m.dx);  // 0-based left node
+  if (k < 0) return zs[0];
+  if (k >= n - 1) return zs[n - 1];
+  double w = (px - xs[k]) / m.dx;
+  w = std::min(1.0, std::max(0.0, w));
+  return (1.0 - w) * zs[k] + w * zs[k + 1];
+}
+
+double grid_x(const Model& m, int ix) { return m.x0 + ix * m.dx; }
+double grid_z(const Model& m, int iz) { return iz * m.dx; }
+
+// Bilinear velocity-grid sample one grid step above/below an interface node
+// (propagate2d.f90:1695-1797).  The velocity grid is the resampled grid with
+// the smesh x positions.
+double vel_side(const Model& m, double px, double pzoff) {
+  const int nx = m.nx, nz = m.nz;
+  const double dxv = m.xpos[1] - m.xpos[0];
+  int ivx = (int)std::floor((px - m.xpos[0]) / dxv);
+  ivx = std::max(0, std::min(nx - 2, ivx));
+  const double wx = std::min(1.0, std::max(0.0, (px - m.xpos[ivx]) / dxv));
+  int ivz;
+  double wz;
+  if (pzoff < grid_z(m, 0)) { ivz = 0; wz = 0.0; }
+  else if (pzoff >= grid_z(m, nz - 1)) { ivz = nz - 2; wz = 1.0; }
+  else {
+    for (ivz = 0; ivz < nz - 1; ++ivz)
+      if (pzoff >= grid_z(m, ivz) && pzoff < grid_z(m, ivz + 1)) break;
+    if (ivz >= nz - 1) ivz = nz - 2;
+    const double up = grid_z(m, ivz + 1) - grid_z(m, ivz);
+    wz = up > 0.0 ? (pzoff - grid_z(m, ivz)) / up : 0.0;
+  }
+  wz = std::min(1.0, std::max(0.0, wz));
+  auto V = [&](int a, int b) { return m.vel[m.g(a, b)]; };
+  return (1.0 - wx) * (1.0 - wz) * V(ivx, ivz) + wx * (1.0 - wz) * V(ivx + 1, ivz) +
+         (1.0 - wx) * wz * V(ivx, ivz + 1) + wx * wz * V(ivx + 1, ivz + 1);
+}
+
+void build_interface(Model& m, int k, const double* zs) {
+  Interface& f = m.ifc[k];
+  const int n = m.nx;
+  f.z.assign(zs, zs + n);
+  f.nrm_x.assign(n, 0.0);
+  f.nrm_z.assign(n, 0.0);
+  const std::vector<double>& X = m.xpos;
+  for (int i = 0; i < n; ++i) {
+    double dzdx;
+    if (i > 0 && i < n - 1) dzdx = (f.z[i + 1] - f.z[i - 1]) / (X[i + 1] - X[i - 1]);
+    else if (i == 0 && n >= 2) dzdx = (f.z[1] - f.z[0]) / (X[1] - X[0]);
+    else if (i == n - 1 && n >= 2) dzdx = (f.z[i] - f.z[i - 1]) / (X[i] - X[i - 1]);
+    else dzdx = 0.0;
+    const double len = std::sqrt(1.0 + dzdx * dzdx);
+    f.nrm_x[i] = -dzdx / len;
+    f.nrm_z[i] = 1.0 / len;
+  }
+  // cut cell of node i: the grid cell in column i whose rows bracket z
+  f.izc.assign(n, -1);
+  f.inode_ok.assign(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const double zv = f.z[i];
+    int c = -1;
+    for (int iz = 0; iz < m.nz - 1; ++iz)
+      if (grid_z(m, iz) <= zv && zv < grid_z(m, iz + 1)) { c = iz; break; }
+    if (c < 0) {
+      if (zv <= grid_z(m, 0)) c = 0;
+      if (zv >= grid_z(m, m.nz - 1)) c = m.nz - 2;
+    }
+    f.izc[i] = c;
+    if (c >= 0) {
+      f.inode_ok[i] = (grid_z(m, c) <= zv && zv <= grid_z(m, c + 1)) ? 1 : 0;
+      // only cells inside the grid are registered for neighbour lookups
+      if (i < m.nx - 1 && c < m.nz - 1) m.cell_cut[(size_t)c * m.nx + i] |= (uint8_t)(1u << k);
+    }
+  }
+}
+
+void define_region(Model& m, Region& r, int itop, int ibot) {
+  r.itop = itop;
+  r.ibot = ibot;
+  const int nx = m.nx, nz = m.nz;
+  r.r0.assign(nx, 0);
+  r.r1.assign(nx, -1);
+  r.col_base.assign(nx, 0);
+  int ng = 0, zlo = nz, zhi = -1;
+  for (int ix = 0; ix < nx; ++ix) {
+    const double zt = iface_z_at(m, m.xpos, m.ifc[itop].z, grid_x(m, ix));
+    const double zb = iface_z_at(m, m.xpos, m.ifc[ibot].z, grid_x(m, ix));
+    int a = -1, b = -2;
+    for (int iz = 0; iz < nz; ++iz) {
+      const double z = grid_z(m, iz);
+      if (zt <= z && z <= zb) {
+        if (a < 0) a = iz;
+        b = iz;
+      }
+    }
+    r.col_base[ix] = ng;
+    if (a >= 0) {
+      r.r0[ix] = a;
+      r.r1[ix] = b;
+      ng += b - a + 1;
+      zlo = std::min(zlo, a);
+      zhi = std::max(zhi, b);
+    } else {
+      r.r0[ix] = 0;
+      r.r1[ix] = -1;
+    }
+  }
+  r.ngnode = ng;
+  r.nnode = ng + 2 * nx;
+  if (zhi < 0) { zlo = 0; zhi = 0; }
+  r.z_lo = zlo;
+  r.z_hi = zhi;
+  r.H = zhi - zlo + 1;
+  r.tiles_x = (nx + kTileW - 1) / kTileW;
+  r.tiles_y = (r.H + kTileH - 1) / kTileH;
+  r.pitch = r.tiles_x * kTileW;
+  r.slot_of_node.assign(r.nnode, 0);
+  for (int ix = 0; ix < nx; ++ix)
+    for (int iz = r.r0[ix]; iz <= r.r1[ix]; ++iz) {
+      const size_t gi = m.g(ix, iz);
+      const int id = r.col_base[ix] + (iz - r.r0[ix]);
+      r.slot_of_node[id] = r.slot_grid(ix, iz);
+      m.node_region[gi] = r.id;
+      m.rnode_id[gi] = id + 1;
+    }
+  m.rright[itop].assign(nx, 0);
+  m.rleft[ibot].assign(nx, 0);
+  for (int k = 0; k < nx; ++k) {
+    r.slot_of_node[ng + k] = r.slot_top(k);
+    r.slot_of_node[ng + nx + k] = r.slot_bot(k);
+    m.rright[itop][k] = ng + k + 1;
+    m.rleft[ibot][k] = ng + nx + k + 1;
+  }
+}
+
+bool in_region(const Region& r, int ix, int iz) {
+  return ix >= 0 && ix < (int)r.r0.size() && iz >= r.r0[ix] && iz <= r.r1[ix];
+}
+
+// Region velocity and per-slot codes (velocities_to_region2d semantics for
+// the velocity, propagate2d.f90:1800-1938).
+void finish_region(Model& m, Region& r) {
+  const int nx = m.nx;
+  const size_t ns = r.nslots();
+  r.code.assign(ns, 0);
+  r.vel.assign(ns, 0.0f);
+  r.vel64.assign(ns, 0.0);
+  r.iface_dz.assign((size_t)2 * r.pitch, 0.0f);
+  r.izc_top.assign(r.pitch, -1);
+  r.izc_bot.assign(r.pitch, -1);
+  const Interface& ft = m.ifc[r.itop];
+  const Interface& fb = m.ifc[r.ibot];
+  const uint8_t tbit = (uint8_t)(1u << r.itop), bbit = (uint8_t)(1u << r.ibot);
+  auto cut = [&](int cx, int cz) { return m.cell_cut[(size_t)cz * nx + cx]; };
+  for (int ix = 0; ix < nx; ++ix) {
+    for (int iz = r.r0[ix]; iz <= r.r1[ix]; ++iz) {
+      const int s = r.slot_grid(ix, iz);
+      double v = m.vel[m.g(ix, iz)];
+      if (iz < m.nz - 1 && !in_region(r, ix, iz + 1)) {
+        int k = (int)std::lround((grid_x(m, ix) - m.xpos[0]) / m.dx);
+        k = std::max(0, std::min(nx - 1, k));
+        v = fb.vel_top[k];
+      }
+      if (iz > 0 && !in_region(r, ix, iz - 1)) {
+        int k = (int)std::lround((grid_x(m, ix) - m.xpos[0]) / m.dx);
+        k = std::max(0, std::min(nx - 1, k));
+        v = ft.vel_bot[k];
+      }
+      r.vel[s] = (float)v;
+      r.vel64[s] = v;
+      uint32_t code = kInRegion | kUpdatable;
+      if (m.fully_regular[m.g(ix, iz)]) code |= kFullyRegular;
+      for (int c = 0; c < 4; ++c) {
+        const int cx = ix - (c >= 2 ? 1 : 0), cz = iz - ((c & 1) ? 1 : 0);
+        if (cx < 0 || cx > nx - 2 || cz < 0 || cz > m.nz - 2) continue;
+        code |= cell_exists_bit(c);
+        const uint8_t cc = cut(cx, cz);
+        if (cc) code |= cell_any_bit(c);
+        if (cc & (tbit | bbit)) {
+          code |= cell_irr_bit(c);
+          if ((cc & tbit) && ft.inode_ok[cx]) code |= cell_top_bit(c);
+          if ((cc & bbit) && fb.inode_ok[cx]) code |= cell_bot_bit(c);
+        }
+      }
+      r.code[s] = code;
+    }
+  }
+  for (int side = 0; side < 2; ++side) {
+    const Interface& f = side == 0 ? ft : fb;
+    const int fbit = side == 0 ? r.itop : r.ibot;
+    for (int k = 0; k < nx; ++k) {
+      const int s = side == 0 ? r.slot_top(k) : r.slot_bot(k);
+      r.vel64[s] = side == 0 ? ft.vel_bot[k] : fb.vel_top[k];
+      r.vel[s] = (float)r.vel64[s];
+      uint32_t code = kInRegion | kIfaceNode;
+      const int c = f.izc[k];
+      (side == 0 ? r.izc_top : r.izc_bot)[k] = c;
+      if (c >= 0) r.iface_dz[(size_t)side * r.pitch + k] = (float)(f.z[k] - grid_z(m, c));
+      if (c >= 0 && k < nx - 1) code |= cell_any_bit(0);
+      if (c >= 0 && k < nx - 1 && f.inode_ok[k]) {
+        code |= kUpdatable | cell_irr_bit(0);
+        const uint8_t cc = cut(k, c);
+        if ((cc & tbit) && ft.inode_ok[k]) code |= cell_top_bit(0);
+        if ((cc & bbit) && fb.inode_ok[k]) code |= cell_bot_bit(0);
+      }
+      (void)fbit;
+      r.code[s] = code;
+    }
+  }
+}
+
+}  // namespace
+
+std::string build_model(Model& m, int nx, int nzs, const double* xpos, const double* topo,
+                        const double* zrel, const double* vel, double vwater,
+                        const double* sed_z, const double* moho_z, int iface_inv) {
+  if (nx < 3 || nzs < 2) return "model too small";
+  const double dx = xpos[1] - xpos[0];
+  if (!(dx > 0.0)) return "xpos must increase";
+  m.nx = nx;
+  m.dx = dx;
+  m.x0 = xpos[0];
+  m.tolerance = dx * 0.01;
+  m.vwater = vwater;
+  m.xpos.assign(xpos, xpos + nx);
+  // resample the smesh onto dz = dx rows (invert2d_main.f90:279-340)
+  const double maxtopo = *std::max_element(topo, topo + nx);
+  const double zmax = zrel[nzs - 1] + maxtopo + 5.0;
+  m.nz = (int)std::lround(zmax / dx) + 1;
+  const int nz = m.nz;
+  m.vel.assign((size_t)nx * nz, 0.0);
+  for (int ix = 0; ix < nx; ++ix) {
+    const int iv = std::min(ix, nx - 2);
+    const double wx = std::min(1.0, std::max(0.0, double(ix - iv)));
+    const double zsf = (1.0 - wx) * topo[iv] + wx * topo[iv + 1];
+    for (int iz = 0; iz < nz; ++iz) {
+      const double pz = grid_z(m, iz) - zsf;
+      double v;
+      if (pz < 0.0) v = vwater;
+      else if (pz >= zrel[nzs - 1]) v = vel[(size_t)(nzs - 1) * nx + ix];
+      else {
+        int io = 0;
+        for (io = 0; io < nzs - 1; ++io)
+          if (pz >= zrel[io] && pz < zrel[io + 1]) break;
+        if (io >= nzs - 1) io = nzs - 2;
+        const double wz = (pz - zrel[io]) / (zrel[io + 1] - zrel[io]);
+        v = (1.0 - wz) * vel[(size_t)io * nx + ix] + wz * vel[(size_t)(io + 1) * nx + ix];
+      }
+      m.vel[m.g(ix, iz)] = v;
+    }
+  }
+  m.cell_cut.assign((size_t)nx * nz, 0);
+  std::vector<double> z1(nx, 0.0), z5(nx, zrel[nzs - 1] + maxtopo);
+  build_interface(m, 1, z1.data());
+  build_interface(m, 2, topo);
+  build_interface(m, 3, sed_z);
+  build_interface(m, 4, moho_z);
+  build_interface(m, 5, z5.data());
+  // regions in the reference's definition order (invert2d_main.f90:420-452)
+  m.node_region.assign((size_t)nx * nz, 0);
+  m.rnode_id.assign((size_t)nx * nz, 0);
+  for (int k = 1; k <= 6; ++k) m.reg[k] = Region(), m.reg[k].id = k;
+  for (int k = 1; k <= 4; ++k) define_region(m, m.reg[k], k, k + 1);
+  m.rright[2].clear();
+  m.rleft[5].clear();
+  define_region(m, m.reg[5], 2, 5);
+  define_region(m, m.reg[6], 2, 4);
+  // fully regular: inside some region, no cut cell among the four around it,
+  // not on the grid border (propagate2d.f90:1941-1979)
+  m.fully_regular.assign((size_t)nx * nz, 0);
+  for (int iz = 1; iz < nz - 1; ++iz)
+    for (int ix = 1; ix < nx - 1; ++ix) {
+      if (m.node_region[m.g(ix, iz)] <= 0) continue;
+      bool reg = true;
+      for (int i = 0; i <= 1; ++i)
+        for (int j = 0; j <= 1; ++j)
+          if (m.cell_cut[(size_t)(iz - j) * nx + (ix - i)]) reg = false;
+      m.fully_regular[m.g(ix, iz)] = reg ? 1 : 0;
+    }
+  for (int k = 1; k <= 5; ++k) {
+    Interface& f = m.ifc[k];
+    f.vel_top.assign(nx, 0.0);
+    f.vel_bot.assign(nx, 0.0);
+    for (int i = 0; i < nx; ++i) {
+      f.vel_top[i] = vel_side(m, m.xpos[i], f.z[i] - dx);
+      f.vel_bot[i] = vel_side(m, m.xpos[i], f.z[i] + dx);
+    }
+  }
+  for (int k = 1; k <= 6; ++k) finish_region(m, m.reg[k]);
+  // inversion numbering: velocity nodes at or below the seafloor, iz outer
+  // (frechet2d.f90:55-63, invert2d_main.f90:456-477)
+  m.inv_idx.assign((size_t)nx * nz, 0);
+  int np = 0;
+  for (int iz = 0; iz < nz; ++iz)
+    for (int ix = 0; ix < nx; ++ix) {
+      const int iv = std::min(ix, nx - 2);
+      const double wx = std::min(1.0, std::max(0.0, double(ix - iv)));
+      const double zsf = (1.0 - wx) * topo[iv] + wx * topo[iv + 1];
+      if (grid_z(m, iz) - zsf >= 0.0) m.inv_idx[m.g(ix, iz)] = ++np;
+    }
+  m.n_vel_parms = np;
+  m.iface_inv = iface_inv;
+  m.n_inv_parms = np + (iface_inv > 0 ? nx : 0);
+  return std::string();
+}
+
+}  // namespace fmt2d

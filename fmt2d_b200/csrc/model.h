@@ -27,8 +27,10 @@ constexpr int kTileH = 32;   // tile height (rows)
 //   bits 8-11  cell is cut by the region's own top/bottom interface
 //   bits 12-15 that cut cell carries a top-interface inode
 //   bits 16-19 that cut cell carries a bottom-interface inode
+//   bits 20-23 cell is cut by any interface (used by the gradient fit)
 // Interface slots: bits 8 (own cut cell irregular), 12/16 (top/bottom inodes
-// present in that cell); the cell's top row is in Region::izc_top/izc_bot.
+// present in that cell), 20 (cell registered); the cell's top row is in
+// Region::izc_top/izc_bot.
 enum : uint32_t {
   kInRegion = 1u << 0,
   kUpdatable = 1u << 1,
@@ -39,6 +41,7 @@ inline uint32_t cell_exists_bit(int c) { return 1u << (4 + c); }
 inline uint32_t cell_irr_bit(int c) { return 1u << (8 + c); }
 inline uint32_t cell_top_bit(int c) { return 1u << (12 + c); }
 inline uint32_t cell_bot_bit(int c) { return 1u << (16 + c); }
+inline uint32_t cell_any_bit(int c) { return 1u << (20 + c); }
 
 struct Interface {
   std::vector<double> z;          // node depth (node ix sits on grid column ix)
@@ -57,6 +60,7 @@ struct Region {
   std::vector<int> col_base;                 // node id of the column's first node - 1
   std::vector<uint32_t> code;                // per slot
   std::vector<float> vel;                    // per slot
+  std::vector<double> vel64;                 // per slot, FP64 (coupling arithmetic)
   std::vector<float> iface_dz;               // per interface slot (2*pitch): z - z(izc)
   std::vector<int> izc_top, izc_bot;         // cut-cell rows of the two interfaces
   std::vector<int> slot_of_node;             // region node id (0-based) -> slot

@@ -1,0 +1,102 @@
+/* fmt2d_gpu.h — C ABI of the B200 implementation of FMT2D's forward-and-
+ * sensitivity path.
+ *
+ * The reference keeps this path behind Fortran subroutine calls on derived
+ * types with pointer components (not C-interoperable).  Each entry point below
+ * replaces one of them for a caller that passes plain contiguous arrays (a
+ * Fortran bind(C) interface module or Python ctypes):
+ *
+ *   fmt2d_upload_model   <- the model build of invert2d_main.f90:139-500
+ *                           (read_smesh outputs + the two interface files);
+ *                           builds find_intersection2d / define_region2d /
+ *                           tag_regular_nodes2d / velocities_to_*2d state
+ *                           (src/propagate2d.f90:1335-1979) on the device
+ *   fmt2d_forward        <- the per-source stage loop of run_forward2d
+ *                           (src/inversion2d.f90:4184-4476): initialize_region_
+ *                           from_source2d, transfer_times_to_intersection,
+ *                           reflect_gradient_at_interface, sweep_region_from_
+ *                           interface2d and propagate2d (interface block
+ *                           src/mod_fmt2d.f90:706-712) for every source
+ *   fmt2d_get_field      <- reading tf%arrivaltime / tf%time_gradient
+ *                           (src/mod_fmt2d.f90:262-279) in region node order
+ *
+ * Conventions: every function returns 0 on success and a negative FMT2D_ERR_*
+ * code on failure (never exits the process); fmt2d_last_error() returns the
+ * message of the last failure on that context.  Region node ids, phase ids
+ * (1 Pg, 2 PsedP, 3 PmP, 4 Pg_ss, 5 Pg_ss2) and time-field ids (1..12) follow
+ * the reference's numbering.  One context per host thread; calls on a context
+ * are ordered on its CUDA stream.  All arrays are caller-owned host memory.
+ */
+#ifndef FMT2D_GPU_H
+#define FMT2D_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FMT2D_API __attribute__((visibility("default")))
+#else
+#define FMT2D_API
+#endif
+
+#define FMT2D_OK 0
+#define FMT2D_ERR_ARG (-1)      /* invalid argument */
+#define FMT2D_ERR_CUDA (-2)     /* CUDA runtime failure or no device */
+#define FMT2D_ERR_STATE (-3)    /* call out of order (e.g. no model uploaded) */
+#define FMT2D_ERR_MODEL (-4)    /* model rejected by the geometry build */
+
+typedef struct fmt2d_ctx fmt2d_ctx;
+
+/* Smesh-level model description (what read_smesh and read_refl return).
+ * vel is nzs rows of nx values (row iz holds depth zrel[iz] below the
+ * seafloor); sed_z and moho_z are interface depths at xpos.  Interface nodes
+ * must sit on the propagation-grid columns (the reference's find_intersection2d
+ * uses the interface index as the grid column). */
+typedef struct fmt2d_model_desc {
+  int nx;                 /* smesh / grid columns */
+  int nzs;                /* smesh depth samples */
+  const double* xpos;     /* [nx] km, uniform spacing = propagation dx = dz */
+  const double* topo;     /* [nx] seafloor depth, km */
+  const double* zrel;     /* [nzs] depth below the seafloor, km */
+  const double* vel;      /* [nzs*nx] P velocity, km/s */
+  double vwater;          /* water velocity, km/s */
+  const double* sed_z;    /* [nx] sediment base depth (interface 3) */
+  const double* moho_z;   /* [nx] Moho depth (interface 4) */
+  int iface_inv;          /* inverted interface for Frechet rows (4 = Moho, 0 none) */
+} fmt2d_model_desc;
+
+/* Context on CUDA device `device` (owns device buffers and one stream).
+ * device = -1 makes a host-only context: the model build and its tables work,
+ * every call that needs the GPU returns FMT2D_ERR_STATE. */
+FMT2D_API int fmt2d_ctx_create(fmt2d_ctx** out, int device);
+FMT2D_API int fmt2d_ctx_destroy(fmt2d_ctx* ctx);
+/* Message of the last failure on ctx (empty if none); writes at most len bytes. */
+FMT2D_API int fmt2d_last_error(fmt2d_ctx* ctx, char* buf, int len);
+
+FMT2D_API int fmt2d_upload_model(fmt2d_ctx* ctx, const fmt2d_model_desc* desc);
+/* Grid size after the dz = dx resampling (invert2d_main.f90:242-246). */
+FMT2D_API int fmt2d_model_info(fmt2d_ctx* ctx, int* nx, int* nz, double* dx, double* x0);
+/* Region r (1..6): node count and, when arrays are given, the reference's node
+ * table (i1 = grid column 1-based or 0 for interface nodes, i2 = grid row
+ * 1-based or interface id, i3 = interface node index 1-based or 0). */
+FMT2D_API int fmt2d_region_nodes(fmt2d_ctx* ctx, int region, int* nnode, int* i1, int* i2, int* i3);
+/* Inversion parameter numbering (frechet2d.f90:55-63): inv_idx[nx*nz] with ix
+ * fastest, 1-based ids, 0 inactive; returns counts. */
+FMT2D_API int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* n_vel_parms, int* n_inv_parms);
+
+/* Solve every time field of the enabled phases (bit p-1 of phase_mask enables
+ * phase p) for nsrc OBS sources placed on the seafloor below src_x[s]. */
+FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask);
+/* Time field tf (1..12) of source s in its region's node order, FP64; any of
+ * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
+FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
+/* Solver counters of the last fmt2d_forward: relaxation rounds, stage batches,
+ * final gradient passes, tile visits and device milliseconds of the rounds. */
+FMT2D_API int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* final_passes,
+                                  long long* tile_visits, double* round_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMT2D_GPU_H */
