@@ -118,7 +118,10 @@ class Fmt2d:
 
     def stats(self):
         a, b, c, v, ms = C.c_int(), C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        ctr = np.zeros(4, np.uint64)
         self._check(self.L.fmt2d_forward_stats(self.h, C.byref(a), C.byref(b), C.byref(c),
-                                               C.byref(v), C.byref(ms)), "fmt2d_forward_stats")
+                                               C.byref(v), C.byref(ms), N.ptr(ctr)),
+                    "fmt2d_forward_stats")
         return dict(rounds=a.value, batches=b.value, final_passes=c.value, tile_visits=v.value,
-                    round_ms=round(ms.value, 3))
+                    round_ms=round(ms.value, 3), passes=int(ctr[0]), steps=int(ctr[1]),
+                    capped=int(ctr[2]), updates=int(ctr[3]))

@@ -141,7 +141,7 @@ int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, doub
 }
 
 int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* finals,
-                        long long* visits, double* round_ms) {
+                        long long* visits, double* round_ms, unsigned long long* counters) {
   if (!ctx) return FMT2D_ERR_ARG;
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
@@ -151,6 +151,12 @@ int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* finals,
   if (finals) *finals = s.final_passes;
   if (visits) *visits = s.tile_visits;
   if (round_ms) *round_ms = s.round_ms;
+  if (counters) {
+    counters[0] = s.passes;
+    counters[1] = s.steps;
+    counters[2] = s.capped;
+    counters[3] = s.updates;
+  }
   return FMT2D_OK;
 }
 

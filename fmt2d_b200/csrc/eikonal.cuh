@@ -31,7 +31,12 @@ struct DevField {
   float* Tl = nullptr;               // time, low part (T = Th + Tl)
   float* gx = nullptr;               // gradient during the solve
   float* gz = nullptr;
-  unsigned* act = nullptr;           // 2 * ntiles round flags
+  unsigned* act = nullptr;           // per tile kTileWords words: active-node masks
+                                     // (32 rows, then top and bottom interface rows)
+  unsigned* tkey = nullptr;          // per tile: smallest pending time (float bits)
+  unsigned* tvis = nullptr;          // per tile: visits so far in this solve
+  float* front = nullptr;            // this field's current front time (device scalar)
+  float band = 1.0f;                 // width of the processing band, seconds
   float4* seed = nullptr;            // per slot: seeded (time hi, lo, gradient) or huge
   uint8_t* sflag = nullptr;          // per slot: bit 0 seeded, bit 1 value copied from a
                                      // coincident node
@@ -42,15 +47,22 @@ struct DevField {
 // A time change above this many seconds is propagated to neighbouring tiles;
 // smaller changes are kept locally (the parity tolerance is 0.5 ms).
 constexpr float kSigDT = 1.0e-6f;
-// Changes above this re-activate the stencil neighbours inside a tile.
-constexpr double kLocalDT = 1.0e-8;
+// Changes above this re-activate the stencil neighbours inside a tile (an
+// order above the FP32 rounding of a re-evaluated time offset).
+constexpr double kLocalDT = 1.0e-7;
 
-// Tile activation bits: why a tile must be visited.
-enum : unsigned {
-  kActAll = 1u,            // seeded, unconverged or flagged by the final pass
-  kActTop = 2u, kActBot = 4u, kActLeft = 8u, kActRight = 16u,
-  kActTL = 32u, kActTR = 64u, kActBL = 128u, kActBR = 256u,
-};
+// A tile visited more often than this in one solve only takes decreases from
+// then on.  The replacement iteration can cycle where the second-order switch
+// of two nodes depends on each other's gradients; taking decreases only ends
+// such a cycle at its lower values.
+constexpr unsigned kMonoVisits = 64;
+
+constexpr int kTileWords = kTH + 2;      // active masks stored per tile
+constexpr unsigned kKeyNone = 0x7f800000u; // +inf: no pending node
 constexpr uint8_t kFlagSeed = 1, kFlagCopy = 2;
+
+__device__ __forceinline__ unsigned key_of(float t) {
+  return t >= kReachedF ? kKeyNone : __float_as_uint(fmaxf(t, 0.0f));
+}
 
 }  // namespace fmt2d

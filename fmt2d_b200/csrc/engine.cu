@@ -85,11 +85,16 @@ double seafloor_at(const Model& m, double px) {
 Engine::Engine(int device) : device_(device) {
   cudaSetDevice(device_);
   cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
-  cudaMallocHost(&h_count_, sizeof(unsigned));
-  cudaFuncSetAttribute(eik_round, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaMallocHost(&h_count_, 4 * sizeof(unsigned));
+  cudaFuncSetAttribute(eik_visit, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)eik_round_smem());
   cudaFuncSetAttribute(eik_final, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)eik_round_smem());
+  // persistent visit blocks: as many warps as fit on the device at once
+  int nsm = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eik_visit, 32, eik_round_smem());
+  visit_blocks_ = std::max(1, nsm) * std::max(1, per_sm);
 }
 
 Engine::~Engine() {
@@ -152,6 +157,11 @@ std::string Engine::upload(const Model& m) {
     X.nz = m.nz;
     D.nslots = G.nslots();
     D.ntiles = G.tiles_x * G.tiles_y;
+    double vs = 0.0;
+    long nv = 0;
+    for (size_t s = 0; s < G.vel64.size(); ++s)
+      if (G.vel64[s] > 0.0) { vs += G.vel64[s]; ++nv; }
+    D.vmean = nv ? vs / nv : 1.0;
   }
   for (int k = 1; k <= 5; ++k) {
     const Interface& f = m.ifc[k];
@@ -233,10 +243,13 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
       F.g2.alloc(D.nslots * 8);
       F.gout.alloc(D.nslots * 8);
       F.susp.alloc(D.nslots);
-      F.act.alloc((size_t)2 * D.ntiles * 4);
+      F.act.alloc((size_t)kTileWords * D.ntiles * 4);
+      F.tkey.alloc((size_t)D.ntiles * 8);   // keys, then visit counts
+      F.front.alloc(16);
       F.seed.alloc(D.nslots * 16);
       F.sflag.alloc(D.nslots);
-      if (!F.t2.p || !F.g2.p || !F.gout.p || !F.susp.p || !F.act.p || !F.seed.p || !F.sflag.p)
+      if (!F.t2.p || !F.g2.p || !F.gout.p || !F.susp.p || !F.act.p || !F.seed.p || !F.sflag.p ||
+          !F.tkey.p || !F.front.p)
         return "device allocation failed for the time fields";
     }
   }
@@ -275,6 +288,10 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     f.gx = F.g2.as<float>();
     f.gz = f.gx;
     f.act = F.act.as<unsigned>();
+    f.tkey = F.tkey.as<unsigned>();
+    f.tvis = f.tkey + reg_[kTf[tf].reg].ntiles;
+    f.front = F.front.as<float>();
+    f.band = (float)(band_tiles * kTW * m_.dx / D.vmean);
     f.seed = F.seed.as<float4>();
     f.sflag = F.sflag.as<uint8_t>();
     f.frozen_slot = -1;
@@ -335,37 +352,59 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     CK(cudaGetLastError());
   }
   d_count_.alloc(16);
+  d_counters_.alloc(4 * sizeof(unsigned long long));
+  unsigned long long* dctr = d_counters_.as<unsigned long long>();
+  CK(cudaMemsetAsync(dctr, 0, 4 * sizeof(unsigned long long), stream_));
   unsigned* dcount = d_count_.as<unsigned>();
   const size_t smem = eik_round_smem();
-  int parity = 0;
+  d_queue_.alloc((size_t)total_tiles * sizeof(unsigned));
+  unsigned* dq = d_queue_.as<unsigned>();
+  {
+    const int bx = (int)std::min<size_t>(((size_t)kTileWords * 4096 + 255) / 256, 256);
+    k_seed_masks<<<dim3(bx, nf), 256, 0, stream_>>>(dF, nf);
+    CK(cudaGetLastError());
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   for (int pass = 0; pass < 6; ++pass) {
     for (int round = 0; round < max_rounds; ++round) {
-      CK(cudaMemsetAsync(dcount, 0, sizeof(unsigned), stream_));
+      // dcount: [0] tiles with pending work, [1] queued tiles, [2] queue head
+      CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
+      eik_front<<<nf, 256, 0, stream_>>>(dF, nf, dcount);
+      eik_select<<<(total_tiles + 255) / 256, 256, 0, stream_>>>(dF, nf, total_tiles, dq,
+                                                                 dcount + 1);
       cudaEventRecord(e0, stream_);
-      eik_round<<<total_tiles, 32, smem, stream_>>>(dF, nf, parity, dcount, max_passes);
+      eik_visit<<<visit_blocks_, 32, smem, stream_>>>(dF, nf, dq, dcount + 1, dcount + 2,
+                                                      max_passes, dctr);
       cudaEventRecord(e1, stream_);
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(h_count_, dcount, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      CK(cudaMemcpyAsync(h_count_, dcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                         stream_));
       CK(cudaStreamSynchronize(stream_));
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, e0, e1);
       stats_.round_ms += ms;
       ++stats_.rounds;
-      stats_.tile_visits += *h_count_;
-      parity ^= 1;
-      if (*h_count_ == 0u) break;
+      stats_.tile_visits += h_count_[1];
+      if (h_count_[0] == 0u) break;
     }
-    CK(cudaMemsetAsync(dcount, 0, sizeof(unsigned), stream_));
+    CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
     eik_final<<<total_tiles, 32, smem, stream_>>>(dF, nf, d_gout_.as<float*>(),
-                                                  d_susp_.as<uint8_t*>(), parity, dcount);
+                                                  d_susp_.as<uint8_t*>(), dcount);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_count_, dcount, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     ++stats_.final_passes;
-    if (*h_count_ == 0u) break;
+    if (h_count_[0] == 0u) break;
+  }
+  {
+    unsigned long long c[4];
+    CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
+    stats_.passes += c[0];
+    stats_.steps += c[1];
+    stats_.capped += c[2];
+    stats_.updates += c[3];
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -35,10 +35,11 @@ struct DevRegionStore {
   DevRegionX X;
   size_t nslots = 0;
   int ntiles = 0;
+  double vmean = 1.0;   // mean region velocity (sets the processing band)
 };
 
 struct FieldStore {
-  DevBuf t2, g2, gout, susp, act, seed, sflag;
+  DevBuf t2, g2, gout, susp, act, seed, sflag, tkey, front;
   bool solved = false;
 };
 
@@ -46,6 +47,9 @@ struct SolveStats {
   int rounds = 0, batches = 0, final_passes = 0;
   long long tile_visits = 0;
   double round_ms = 0.0;     // device time of the round kernels
+  // device counters: sweep passes, warp row/column steps, visits that hit
+  // the pass cap, node updates
+  unsigned long long passes = 0, steps = 0, capped = 0, updates = 0;
 };
 
 class Engine {
@@ -61,6 +65,7 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
   const SolveStats& stats() const { return stats_; }
   int max_passes = 64;     // directional sweeps per tile visit before it re-queues itself
+  double band_tiles = 1.5; // processing band: this many tile widths at the mean velocity
   int max_rounds = 4000;   // safety cap on rounds per batch
   // device pointers of a solved field (float2 time, float2 gradient per slot)
   const float* field_t(int src, int tf) const { return fields_[src][tf].t2.as<float>(); }
@@ -83,8 +88,9 @@ class Engine {
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
   DevBuf d_fields_, d_xs_, d_seeds_, d_sx_, d_sz_, d_count_, d_gout_, d_susp_, d_up_, d_which_,
-      d_scratch_;
+      d_scratch_, d_counters_, d_queue_;
   unsigned* h_count_ = nullptr;
+  int visit_blocks_ = 1;
   SolveStats stats_;
 };
 

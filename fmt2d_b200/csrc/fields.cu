@@ -17,16 +17,22 @@ __device__ __forceinline__ double tdbl(float2 t) {
   return t.x >= kReachedF ? 1.0e20 : (double)t.x + (double)t.y;
 }
 
-__device__ __forceinline__ void mark_grid(const DevField& F, int col, int brow) {
+// A seeded node lowers the key of its tile and of the tiles whose halo holds
+// it; k_seed_masks then opens every node of the tiles with a key.
+__device__ __forceinline__ void mark_grid(const DevField& F, int col, int brow, float t) {
   const DevRegion& R = F.R;
-  F.act[(size_t)(brow / kTH) * R.tiles_x + col / kTW] = 1u;
+  const unsigned key = key_of(t);
+  const int tx0 = max(0, (col - kHalo) / kTW), tx1 = min(R.tiles_x - 1, (col + kHalo) / kTW);
+  const int ty0 = max(0, (brow - kHalo) / kTH), ty1 = min(R.tiles_y - 1, (brow + kHalo) / kTH);
+  for (int ty = ty0; ty <= ty1; ++ty)
+    for (int tx = tx0; tx <= tx1; ++tx) atomicMin(F.tkey + ty * R.tiles_x + tx, key);
 }
 
-__device__ __forceinline__ void mark_iface(const DevField& F, int side, int col) {
+__device__ __forceinline__ void mark_iface(const DevField& F, int side, int col, float t) {
   const DevRegion& R = F.R;
   int row = R.izc[side * R.pitch + col] - R.z_lo;
   row = row < 0 ? 0 : (row >= R.H ? R.H - 1 : row);
-  mark_grid(F, col, row);
+  mark_grid(F, col, row, t);
 }
 
 // rays-free fit of the time gradient at one node (propagate2d.f90:949-1196).
@@ -138,7 +144,8 @@ __global__ void k_fill(DevField* fields, int nf, size_t max_slots) {
   DevField& F = fields[fi];
   const size_t ns = (size_t)(F.R.H + 2) * F.R.pitch;
   const int nt = F.R.tiles_x * F.R.tiles_y;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns || i < (size_t)2 * nt;
+  const size_t nw = (size_t)kTileWords * nt;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns || i < nw;
        i += (size_t)gridDim.x * blockDim.x) {
     if (i < ns) {
       reinterpret_cast<float2*>(F.Th)[i] = make_float2(kHugeF, 0.0f);
@@ -146,9 +153,13 @@ __global__ void k_fill(DevField* fields, int nf, size_t max_slots) {
       F.seed[i] = make_float4(kHugeF, 0.0f, 0.0f, 0.0f);
       F.sflag[i] = 0;
     }
-    if (i < (size_t)2 * nt) F.act[i] = 0u;
+    if (i < nw) F.act[i] = 0u;
+    if (i < (size_t)nt) { F.tkey[i] = kKeyNone; F.tvis[i] = 0u; }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) F.frozen_slot = -1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    F.frozen_slot = -1;
+    *F.front = kHugeF;
+  }
   (void)max_slots;
 }
 
@@ -190,7 +201,7 @@ __global__ void k_init_source(DevField* fields, const DevRegionX* xs, const doub
       reinterpret_cast<float2*>(F.gx)[s] = g;
       F.seed[s] = make_float4(t.x, t.y, g.x, g.y);
       F.sflag[s] = 1;
-      mark_grid(F, ix, br);
+      mark_grid(F, ix, br, t.x);
     }
 }
 
@@ -238,7 +249,7 @@ __global__ void k_seed_iface(const SeedDesc* descs, int nd, int nz) {
     reinterpret_cast<float2*>(D.dst.gx)[s] = make_float2((float)gx, (float)gz);
     D.dst.seed[s] = make_float4(t.x, t.y, (float)gx, (float)gz);
     D.dst.sflag[s] = 1;
-    mark_iface(D.dst, D.dst_side, c);
+    mark_iface(D.dst, D.dst_side, c, t.x);
   }
   // grid nodes of column c: the first interface node (c-1, c, c+1) whose
   // three-row box holds a node seeds it
@@ -274,7 +285,7 @@ __global__ void k_seed_iface(const SeedDesc* descs, int nd, int nz) {
       reinterpret_cast<float2*>(D.dst.gx)[s] = gs;
       D.dst.seed[s] = make_float4(t.x, t.y, gs.x, gs.y);
       D.dst.sflag[s] = 1;
-      mark_grid(D.dst, c, br);
+      mark_grid(D.dst, c, br, t.x);
     }
   }
 }
@@ -377,6 +388,15 @@ __global__ void k_export(const float* t2, const float* g2, const int* slot_of_no
     if (gx) gx[n] = g.x;
     if (gz) gz[n] = g.y;
   }
+}
+
+// Every node of a seeded tile (one with a key after seeding) starts active.
+__global__ void k_seed_masks(DevField* fields, int nf) {
+  const DevField& F = fields[blockIdx.y];
+  const int nt = F.R.tiles_x * F.R.tiles_y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt * kTileWords;
+       i += gridDim.x * blockDim.x)
+    if (F.tkey[i / kTileWords] != kKeyNone) F.act[i] = 0xffffffffu;
 }
 
 }  // namespace fmt2d

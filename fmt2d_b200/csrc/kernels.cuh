@@ -4,11 +4,16 @@
 
 namespace fmt2d {
 
-__global__ void eik_round(const DevField* fields, int nf, int parity, unsigned* n_next,
-                          int max_passes);
+__global__ void eik_front(const DevField* fields, int nf, unsigned* n_pending);
+__global__ void eik_select(const DevField* fields, int nf, int total_tiles, unsigned* queue,
+                           unsigned* qlen);
+__global__ void eik_visit(const DevField* fields, int nf, const unsigned* queue,
+                          const unsigned* qlen, unsigned* qhead, int max_passes,
+                          unsigned long long* counters);
 __global__ void eik_final(const DevField* fields, int nf, float* const* gout,
-                          uint8_t* const* susp, int parity, unsigned* n_bad);
+                          uint8_t* const* susp, unsigned* n_bad);
 size_t eik_round_smem();
+__global__ void k_seed_masks(DevField* fields, int nf);
 
 __global__ void k_fill(DevField* fields, int nf, size_t max_slots);
 __global__ void k_init_source(DevField* fields, const DevRegionX* xs, const double* sx,

@@ -92,9 +92,11 @@ FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int p
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
 /* Solver counters of the last fmt2d_forward: relaxation rounds, stage batches,
- * final gradient passes, tile visits and device milliseconds of the rounds. */
+ * final gradient passes, tile visits, device milliseconds of the rounds, and
+ * (counters[4]) sweep passes, warp sweep steps, capped visits, node updates. */
 FMT2D_API int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* final_passes,
-                                  long long* tile_visits, double* round_ms);
+                                  long long* tile_visits, double* round_ms,
+                                  unsigned long long* counters);
 
 #ifdef __cplusplus
 }
