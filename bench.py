@@ -1,0 +1,358 @@
+"""Throughput of the FMT2D forward hot path on B200: eikonal time fields per second.
+
+Workload (one step): every OBS source x every stage of the Pg and PmP phases of
+the joint velocity + Moho model, 2001 x 401 nodes at 0.1 km (30 OBS every
+6.5 km; Pg = 1 field, PmP = 2 stages down to the Moho and back up), i.e. 90
+eikonal time fields, solved through the library's public entry point.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value  : fields/s with the model resident on the device (device-timed with
+           CUDA events on the library's stream, max over ranks).
+* e2e    : the same metric through the public API from host buffers: model
+           upload (host arrays -> device), the forward solve, and the read-back
+           of every terminal-stage traveltime field to host memory.
+* roofline: the relaxation kernel against the measured HBM bandwidth, with the
+           algorithmic traffic of one field (16 B per region node: time and
+           gradient written once, velocity and geometry code read once).
+* cpu_baseline: the FP64 CPU restatement of the reference algorithm (oracle/)
+           on the host cores, over a bounded sample of the same workload.
+* --impl reference: the CPU restatement timed on all host cores (the reference
+           Fortran cannot be built here: no Fortran compiler in the image).
+
+Multi-GPU: one process per GPU (torchrun); every rank solves its own copy of
+the workload (independent source sets), no collective on the data path
+(weak scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+PHASES = (1, 3)          # Pg, PmP
+WORKLOAD = "fmt2d forward, 2001x401 joint velocity+Moho model, 30 OBS, Pg+PmP (90 fields)"
+METRIC = "eikonal fields/s @2001x401 (<=0.5 ms err)"
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+# ---------------------------------------------------------------- CPU arms
+_CPU_STATE = {}
+
+
+def _cpu_init():
+    if "o" not in _CPU_STATE:
+        sys.path.insert(0, os.path.join(HERE, "oracle"))
+        import pyoracle
+        from fmt2d_b200 import synth
+        m = synth.config(1)
+        _CPU_STATE.update(m=m, o=pyoracle.Oracle(m))
+
+
+def _cpu_worker(args):
+    """One process of the CPU restatement: solve the given sources, return seconds.
+    The model is generated and built once per process, outside the timing."""
+    src_idx, phases = args
+    _cpu_init()
+    from fmt2d_b200.api import phase_mask
+    m, o = _CPU_STATE["m"], _CPU_STATE["o"]
+    mask = phase_mask(phases)
+    t0 = time.perf_counter()
+    for s in src_idx:
+        o.forward(0, float(m.obs_x[s]), mask)
+    return time.perf_counter() - t0
+
+
+def cpu_fields_per_s(nsrc: int, procs: int, reps: int = 1):
+    """Fields/s of the CPU restatement over `nsrc` sources on `procs` processes."""
+    from fmt2d_b200.api import fields_of, phase_mask
+    nf_src = len(fields_of(phase_mask(PHASES)))
+    ctx = mp.get_context("spawn")
+    chunks = [list(range(i, nsrc, procs)) for i in range(procs)]
+    chunks = [c for c in chunks if c]
+    with ctx.Pool(len(chunks), initializer=_cpu_init) as pool:
+        walls = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
+            walls.append(time.perf_counter() - t0)
+    return nsrc * nf_src / float(np.median(walls)), len(chunks), walls
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if len(r) >= 8 and num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if len(r) >= 8 and num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 8
+                          for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peak_hbm():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        for k in ("hbm_gbs", "hbm_GBps", "hbm"):
+            if k in d:
+                return float(d[k]), "measured"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback"
+
+
+def dist_setup(n_gpus):
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- arms
+def run_reference(args, world, rank):
+    """CPU restatement of the reference path on all host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from fmt2d_b200 import synth
+    from fmt2d_b200.api import fields_of, phase_mask
+    cores = os.cpu_count() or 1
+    m = synth.config(1)
+    nsrc_all = len(m.obs_x)
+    # each step: a bounded sample of the workload (sources spread over the cores)
+    nsrc = min(nsrc_all, max(cores, 4))
+    nf_src = len(fields_of(phase_mask(PHASES)))
+    ctx = mp.get_context("spawn")
+    procs = min(cores, nsrc)
+    chunks = [list(range(i, nsrc, procs)) for i in range(procs)]
+    walls = []
+    with ctx.Pool(procs, initializer=_cpu_init) as pool:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
+            if step >= args.warmup:
+                walls.append(time.perf_counter() - t0)
+    sec = float(np.sum(walls))
+    value = nsrc * nf_src * len(walls) / sec
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "fields/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(1e3 * sec / len(walls), 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "sample_sources": nsrc, "fields_per_step":
+                      nsrc * nf_src},
+           "cpu_baseline": {"value": round(value, 3), "unit": "fields/s", "cores": procs,
+                            "kind": "port",
+                            "sample": f"{nsrc} of {nsrc_all} sources x Pg+PmP stages per step, "
+                                      f"FP64 heap fast marching, {procs} processes"},
+           "e2e": {"value": round(value, 3), "unit": "fields/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0},
+           "gpu_launches": 0}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # before the first CUDA call: the CPU restatement on the host cores
+        cores = os.cpu_count() or 1
+        nsrc = min(30, max(4, cores))
+        procs = min(cores, nsrc)
+        v, used, walls = cpu_fields_per_s(nsrc, procs)
+        cpu = {"value": round(v, 3), "unit": "fields/s", "cores": used, "kind": "port",
+               "sample": f"{nsrc} sources x Pg+PmP stages of the same model, FP64 heap fast "
+                         f"marching, {used} processes, {walls[0]:.1f} s wall"}
+    import torch
+    from fmt2d_b200 import synth
+    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask, TF_REGION
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    m = synth.config(1)
+    g = Fmt2d(local).upload(m)
+    stream = torch.cuda.ExternalStream(g.stream(), device=dev)
+    src = np.asarray(m.obs_x, dtype=np.float64)
+    mask = phase_mask(PHASES)
+    nf = len(fields_of(mask)) * src.size
+    terminal = [1, 5]          # last stage of Pg and of PmP (ray tracing starts there)
+
+    for _ in range(args.warmup):
+        g.forward(src, PHASES)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    solve_ms, launches, nodes = 0.0, 0, 0
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.forward(src, PHASES)
+            st = g.stats()
+            solve_ms += st["solve_ms"]
+            launches += st["launches"]
+            nodes += st["nodes"]
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms, world, dev)
+    step_ms = ms / args.steps
+    value = world * nf / (step_ms / 1e3)
+
+    # ---- end to end through the public API from host buffers
+    bufs = {}
+    for tf in terminal:
+        n = g.region_nnode(TF_REGION[tf])
+        bufs[tf] = np.zeros(n)
+    h2d = sum(np.asarray(a).nbytes for a in (m.xpos, m.topo, m.zrel, m.vel, m.sed_z, m.moho_z))
+    d2h = sum(src.size * bufs[tf].nbytes for tf in terminal)
+
+    def e2e_step():
+        g.upload(m)
+        g.forward(src, PHASES)
+        for s in range(src.size):
+            for tf in terminal:
+                g._check(g.L.fmt2d_get_field(g.h, s, tf, bufs[tf].ctypes.data, None, None),
+                         "fmt2d_get_field")
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world, dev)
+    e2e_value = world * nf / e2e_s
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak_hbm()
+    alg_bytes = 16.0 * nodes / args.steps          # per step, all fields
+    achieved = alg_bytes / (solve_ms / args.steps / 1e3) / 1e9 if solve_ms > 0 else None
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "fields/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": WORKLOAD, "grid": "2001x401", "sources_per_gpu": int(src.size),
+                      "fields_per_gpu": nf, "l2": "field data per step (> 1 GB) exceeds L2",
+                      "parallelism": f"sources x {world} gpus, independent"},
+           "e2e": {"value": round(e2e_value, 3), "unit": "fields/s", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(d2h), "includes": "model upload, forward, "
+                   "terminal-stage traveltime read-back"},
+           "roofline": {"bound": "hbm", "kernel": "eik_visit",
+                        "achieved": round(achieved, 3) if achieved else None,
+                        "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 6) if achieved else None,
+                        "peak_kind": peak_kind, "traffic": None,
+                        "algorithmic_bytes_per_step": alg_bytes},
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "cpu_baseline": cpu}
+    print(json.dumps(out), flush=True)
+    g.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # host-core arm: rank 0 alone runs it, the other ranks exit without work
+        run_reference(args, _env_int("WORLD_SIZE", 1), _env_int("RANK", 0))
+        return
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -57,8 +57,8 @@ def lib():
     L.fmt2d_inv_index.argtypes = [V, C.c_void_p, P(C.c_int), P(C.c_int)]
     L.fmt2d_forward.argtypes = [V, _dp, C.c_int, C.c_int]
     L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
-    L.fmt2d_forward_stats.argtypes = [V, P(C.c_int), P(C.c_int), P(C.c_int),
-                                      P(C.c_longlong), P(C.c_double), C.c_void_p]
+    L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
+    L.fmt2d_stream.argtypes = [V, P(V)]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int
     _lib = L

@@ -116,12 +116,18 @@ class Fmt2d:
                     "fmt2d_get_field")
         return T, gx, gz
 
-    def stats(self):
-        a, b, c, v, ms = C.c_int(), C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
-        ctr = np.zeros(4, np.uint64)
-        self._check(self.L.fmt2d_forward_stats(self.h, C.byref(a), C.byref(b), C.byref(c),
-                                               C.byref(v), C.byref(ms), N.ptr(ctr)),
-                    "fmt2d_forward_stats")
-        return dict(rounds=a.value, batches=b.value, final_passes=c.value, tile_visits=v.value,
-                    round_ms=round(ms.value, 3), passes=int(ctr[0]), steps=int(ctr[1]),
-                    capped=int(ctr[2]), updates=int(ctr[3]))
+    STATS = ("rounds", "batches", "final_passes", "tile_visits", "solve_ms", "launches",
+             "nodes", "passes", "steps", "capped", "updates")
+
+    def stats(self) -> dict:
+        """Counters of the last forward (fmt2d_stats)."""
+        v = np.zeros(len(self.STATS))
+        self._check(self.L.fmt2d_stats(self.h, N.ptr(v), v.size), "fmt2d_stats")
+        return {k: (round(float(x), 3) if k == "solve_ms" else int(x))
+                for k, x in zip(self.STATS, v)}
+
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) that the context's work runs on."""
+        s = C.c_void_p()
+        self._check(self.L.fmt2d_stream(self.h, C.byref(s)), "fmt2d_stream")
+        return int(s.value or 0)

@@ -140,23 +140,24 @@ int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, doub
   return FMT2D_OK;
 }
 
-int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* finals,
-                        long long* visits, double* round_ms, unsigned long long* counters) {
-  if (!ctx) return FMT2D_ERR_ARG;
+int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
+  if (!ctx || !values || n < 0) return FMT2D_ERR_ARG;
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
   const fmt2d::SolveStats& s = ctx->eng->stats();
-  if (rounds) *rounds = s.rounds;
-  if (batches) *batches = s.batches;
-  if (finals) *finals = s.final_passes;
-  if (visits) *visits = s.tile_visits;
-  if (round_ms) *round_ms = s.round_ms;
-  if (counters) {
-    counters[0] = s.passes;
-    counters[1] = s.steps;
-    counters[2] = s.capped;
-    counters[3] = s.updates;
-  }
+  const double v[FMT2D_N_STATS] = {(double)s.rounds,   (double)s.batches, (double)s.final_passes,
+                                   (double)s.tile_visits, s.round_ms,     (double)s.launches,
+                                   (double)s.nodes,    (double)s.passes,  (double)s.steps,
+                                   (double)s.capped,   (double)s.updates};
+  for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
+  return FMT2D_OK;
+}
+
+int fmt2d_stream(fmt2d_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  *stream = (void*)ctx->eng->stream();
   return FMT2D_OK;
 }
 

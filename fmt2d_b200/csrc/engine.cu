@@ -314,6 +314,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   {
     const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 1024);
     k_fill<<<dim3(bx, nf), 256, 0, stream_>>>(dF, nf, max_slots);
+    ++stats_.launches;
     CK(cudaGetLastError());
   }
   const int level = kTf[items[0].second].level;
@@ -325,6 +326,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     k_init_source<<<(nf + 63) / 64, 64, 0, stream_>>>(dF, d_xs_.as<DevRegionX>(),
                                                        d_sx_.as<double>(), d_sz_.as<double>(),
                                                        nf, m_.nz);
+    ++stats_.launches;
     CK(cudaGetLastError());
   } else {
     std::vector<SeedDesc> sd(nf);
@@ -349,6 +351,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     if (!(e = put(d_seeds_, sd, stream_)).empty()) return e;
     k_seed_iface<<<dim3((m_.nx + 127) / 128, nf), 128, 0, stream_>>>(d_seeds_.as<SeedDesc>(), nf,
                                                                     m_.nz);
+    ++stats_.launches;
     CK(cudaGetLastError());
   }
   d_count_.alloc(16);
@@ -362,6 +365,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   {
     const int bx = (int)std::min<size_t>(((size_t)kTileWords * 4096 + 255) / 256, 256);
     k_seed_masks<<<dim3(bx, nf), 256, 0, stream_>>>(dF, nf);
+    ++stats_.launches;
     CK(cudaGetLastError());
   }
   cudaEvent_t e0, e1;
@@ -372,11 +376,14 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
       // dcount: [0] tiles with pending work, [1] queued tiles, [2] queue head
       CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
       eik_front<<<nf, 256, 0, stream_>>>(dF, nf, dcount);
+      ++stats_.launches;
       eik_select<<<(total_tiles + 255) / 256, 256, 0, stream_>>>(dF, nf, total_tiles, dq,
                                                                  dcount + 1);
+      ++stats_.launches;
       cudaEventRecord(e0, stream_);
       eik_visit<<<visit_blocks_, 32, smem, stream_>>>(dF, nf, dq, dcount + 1, dcount + 2,
                                                       max_passes, dctr);
+      ++stats_.launches;
       cudaEventRecord(e1, stream_);
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(h_count_, dcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
@@ -392,6 +399,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
     eik_final<<<total_tiles, 32, smem, stream_>>>(dF, nf, d_gout_.as<float*>(),
                                                   d_susp_.as<uint8_t*>(), dcount);
+    ++stats_.launches;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_count_, dcount, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -413,9 +421,11 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     k_fit_suspect<<<dim3(bx, nf), 256, 0, stream_>>>(dF, d_xs_.as<DevRegionX>(),
                                                      d_gout_.as<float*>(), d_susp_.as<uint8_t*>(),
                                                      nf);
+    ++stats_.launches;
     CK(cudaGetLastError());
     k_water_fix<<<dim3((m_.nx + 127) / 128, nf), 128, 0, stream_>>>(dF, d_gout_.as<float*>(),
                                                                    d_up_.as<int>(), nf);
+    ++stats_.launches;
     CK(cudaGetLastError());
   }
   if (!hw.empty()) {
@@ -425,10 +435,14 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     k_headwave<<<((int)hw.size() + 31) / 32, 32, 0, stream_>>>(
         dF, d_xs_.as<DevRegionX>(), d_gout_.as<float*>(), hw_slot_.as<int>(), hw_v_.as<double>(),
         dx_if, m_.nx, d_scratch_.as<double>(), d_which_.as<int>(), (int)hw.size());
+    ++stats_.launches;
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(stream_));
-  for (int i = 0; i < nf; ++i) fields_[items[i].first][items[i].second].solved = true;
+  for (int i = 0; i < nf; ++i) {
+    fields_[items[i].first][items[i].second].solved = true;
+    stats_.nodes += m_.reg[kTf[items[i].second].reg].nnode;
+  }
   ++stats_.batches;
   return std::string();
 }
@@ -448,6 +462,7 @@ std::string Engine::get_field(int src, int tf, double* T, double* gx, double* gz
   k_export<<<(nn + 255) / 256, 256, 0, stream_>>>(F.t2.as<float>(), F.gout.as<float>(),
                                                   D.slot_of_node.as<int>(), nn, d, d + nn,
                                                   d + 2 * (size_t)nn);
+  ++stats_.launches;
   CK(cudaGetLastError());
   if (T) CK(cudaMemcpyAsync(T, d, nn * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   if (gx) CK(cudaMemcpyAsync(gx, d + nn, nn * sizeof(double), cudaMemcpyDeviceToHost, stream_));

@@ -50,6 +50,8 @@ struct SolveStats {
   // device counters: sweep passes, warp row/column steps, visits that hit
   // the pass cap, node updates
   unsigned long long passes = 0, steps = 0, capped = 0, updates = 0;
+  long long launches = 0;     // kernels launched since the last forward began
+  long long nodes = 0;        // region nodes of the time fields solved
 };
 
 class Engine {

@@ -91,12 +91,18 @@ FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int p
 /* Time field tf (1..12) of source s in its region's node order, FP64; any of
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
-/* Solver counters of the last fmt2d_forward: relaxation rounds, stage batches,
- * final gradient passes, tile visits, device milliseconds of the rounds, and
- * (counters[4]) sweep passes, warp sweep steps, capped visits, node updates. */
-FMT2D_API int fmt2d_forward_stats(fmt2d_ctx* ctx, int* rounds, int* batches, int* final_passes,
-                                  long long* tile_visits, double* round_ms,
-                                  unsigned long long* counters);
+/* Counters of the last fmt2d_forward (and of the exports since), in this
+ * order: [0] relaxation rounds, [1] stage batches, [2] final gradient passes,
+ * [3] tile visits, [4] device milliseconds of the relaxation kernel, [5] kernel
+ * launches, [6] region nodes of the solved time fields, [7] sweep passes,
+ * [8] warp sweep steps, [9] visits that hit the pass cap, [10] node updates.
+ * Writes min(n, FMT2D_N_STATS) values.  No reference counterpart (diagnostics). */
+#define FMT2D_N_STATS 11
+FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
+
+/* The CUDA stream (cudaStream_t) all work of the context is issued on, for
+ * callers that record events around fmt2d_forward.  No reference counterpart. */
+FMT2D_API int fmt2d_stream(fmt2d_ctx* ctx, void** stream);
 
 #ifdef __cplusplus
 }
