@@ -26,6 +26,12 @@ class ModelDesc(C.Structure):
                 ("sed_z", C.c_void_p), ("moho_z", C.c_void_p), ("iface_inv", C.c_int)]
 
 
+class LsqrParams(C.Structure):
+    _fields_ = [("smooth_type", C.c_int), ("max_iter", C.c_int), ("wdv", C.c_double),
+                ("wdv_iface", C.c_double), ("w_smooth", C.c_double),
+                ("w_smooth_iface", C.c_double), ("eps_min", C.c_double)]
+
+
 class Fmt2dError(RuntimeError):
     pass
 
@@ -59,6 +65,13 @@ def lib():
     L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
+    L.fmt2d_set_frechet.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int]
+    L.fmt2d_spmv.argtypes = [V, C.c_int, C.c_void_p, C.c_void_p]
+    L.fmt2d_gtg_diag.argtypes = [V, C.c_void_p]
+    L.fmt2d_lsqr.argtypes = [V, P(LsqrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             P(C.c_int), P(C.c_double), P(C.c_double), P(C.c_double)]
+    L.fmt2d_lsqr_stats.argtypes = [V, P(C.c_double), P(C.c_int)]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int
     _lib = L

@@ -126,6 +126,53 @@ class Fmt2d:
         return {k: (round(float(x), 3) if k == "solve_ms" else int(x))
                 for k, x in zip(self.STATS, v)}
 
+    # ------------------------------------------------------------ G and LSQR
+    def set_frechet(self, ndata: int, nparm: int, row_ptr, gindx, gval, index_base: int = 1):
+        """Sensitivity matrix as CSR (read_frechet_data2d's gindx / gval /
+        row_ptr, 1-based by default)."""
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        gi = np.ascontiguousarray(gindx, dtype=np.int32)
+        gv = np.ascontiguousarray(gval, dtype=np.float64)
+        if rp.size != ndata + 1:
+            raise ValueError("row_ptr needs ndata + 1 entries")
+        self._check(self.L.fmt2d_set_frechet(self.h, int(ndata), int(nparm), N.ptr(rp), N.ptr(gi),
+                                             N.ptr(gv), int(index_base)), "fmt2d_set_frechet")
+        self.ndata, self.nparm = int(ndata), int(nparm)
+        return self
+
+    def spmv(self, x, transpose: bool = False):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != (self.ndata if transpose else self.nparm):
+            raise ValueError("x has the wrong length")
+        y = np.zeros(self.nparm if transpose else self.ndata)
+        self._check(self.L.fmt2d_spmv(self.h, int(bool(transpose)), N.ptr(x), N.ptr(y)),
+                    "fmt2d_spmv")
+        return y
+
+    def gtg_diag(self):
+        out = np.zeros(self.nparm)
+        self._check(self.L.fmt2d_gtg_diag(self.h, N.ptr(out)), "fmt2d_gtg_diag")
+        return out
+
+    def lsqr(self, residual, dm_sum=None, gtg_diag=None, *, wdv=0.0, wdv_iface=0.0,
+             w_smooth=0.0, w_smooth_iface=0.0, eps_min=0.0, max_iter=2000, smooth_type=1):
+        """run_lsqr on the current G; returns (dm, iters, rnorm, bnorm, test2)."""
+        f = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        r, s, g = f(residual), f(dm_sum), f(gtg_diag)
+        p = N.LsqrParams(int(smooth_type), int(max_iter), float(wdv), float(wdv_iface),
+                         float(w_smooth), float(w_smooth_iface), float(eps_min))
+        dm = np.zeros(self.nparm)
+        it, rn, bn, t2 = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        self._check(self.L.fmt2d_lsqr(self.h, C.byref(p), N.ptr(r), N.ptr(g), N.ptr(s), N.ptr(dm),
+                                      C.byref(it), C.byref(rn), C.byref(bn), C.byref(t2)),
+                    "fmt2d_lsqr")
+        return dm, it.value, rn.value, bn.value, t2.value
+
+    def lsqr_stats(self):
+        ms, n = C.c_double(), C.c_int()
+        self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
+        return {"ms": ms.value, "launches": n.value}
+
     def stream(self) -> int:
         """cudaStream_t (as an integer) that the context's work runs on."""
         s = C.c_void_p()

@@ -1,6 +1,7 @@
 // C ABI entry points (include/fmt2d_gpu.h).
 #include "../../include/fmt2d_gpu.h"
 #include "engine.h"
+#include "lsqr.h"
 #include <cstring>
 #include <memory>
 #include <new>
@@ -8,6 +9,7 @@
 
 struct fmt2d_ctx {
   std::unique_ptr<fmt2d::Engine> eng;   // null for a host-only context
+  std::unique_ptr<fmt2d::Lsqr> lsqr;    // G products and LSQR (device contexts)
   fmt2d::Model model;
   std::string err;
   bool has_model = false;
@@ -39,6 +41,7 @@ int fmt2d_ctx_create(fmt2d_ctx** out, int device) {
   fmt2d_ctx* c = new (std::nothrow) fmt2d_ctx();
   if (!c) return FMT2D_ERR_ARG;
   c->eng.reset(new fmt2d::Engine(device));
+  c->lsqr.reset(new fmt2d::Lsqr(device, c->eng->stream()));
   if (cudaGetLastError() != cudaSuccess) {
     delete c;
     return FMT2D_ERR_CUDA;
@@ -70,6 +73,8 @@ int fmt2d_upload_model(fmt2d_ctx* ctx, const fmt2d_model_desc* d) {
   if (!e.empty()) return ctx->fail(FMT2D_ERR_MODEL, e);
   if (ctx->eng) {
     e = ctx->eng->upload(ctx->model);
+    if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+    e = ctx->lsqr->set_geometry(ctx->model);
     if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
   }
   ctx->has_model = true;
@@ -150,6 +155,78 @@ int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
                                    (double)s.nodes,    (double)s.passes,  (double)s.steps,
                                    (double)s.capped,   (double)s.updates};
   for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
+  return FMT2D_OK;
+}
+
+int fmt2d_set_frechet(fmt2d_ctx* ctx, int ndata, int nparm, const int* row_ptr,
+                      const int* gindx, const double* gval, int index_base) {
+  if (!ctx || !row_ptr || ndata < 0 || nparm <= 0 || (index_base != 0 && index_base != 1))
+    return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const std::string e = ctx->lsqr->set_matrix(ndata, nparm, row_ptr, gindx, gval, index_base);
+  if (!e.empty()) return ctx->fail(e.find("CUDA") != std::string::npos ||
+                                       e.find("allocation") != std::string::npos
+                                       ? FMT2D_ERR_CUDA : FMT2D_ERR_ARG, e);
+  return FMT2D_OK;
+}
+
+int fmt2d_spmv(fmt2d_ctx* ctx, int transpose, const double* x, double* y) {
+  if (!ctx || !x || !y) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
+  const std::string e = ctx->lsqr->spmv(transpose != 0, x, y);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  return FMT2D_OK;
+}
+
+int fmt2d_gtg_diag(fmt2d_ctx* ctx, double* gtg) {
+  if (!ctx || !gtg) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
+  const std::string e = ctx->lsqr->gtg_diag(gtg);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  return FMT2D_OK;
+}
+
+int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residual,
+               const double* gtg_diag, const double* dm_sum, double* dm, int* iters, double* rnorm,
+               double* bnorm, double* test2) {
+  if (!ctx || !p || !dm) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
+  if (p->smooth_type != 1) return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1 (Laplacian)");
+  if (p->max_iter < 1) return ctx->fail(FMT2D_ERR_ARG, "max_iter must be >= 1");
+  if (ctx->lsqr->nparm() != ctx->model.n_inv_parms)
+    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the model's inversion parameters");
+  fmt2d::LsqrParams q;
+  q.smooth_type = p->smooth_type;
+  q.max_iter = p->max_iter;
+  q.wdv = p->wdv;
+  q.wdv_iface = p->wdv_iface;
+  q.w_smooth = p->w_smooth;
+  q.w_smooth_iface = p->w_smooth_iface;
+  q.eps_min = p->eps_min;
+  fmt2d::LsqrOut o;
+  const std::string e = ctx->lsqr->solve(q, residual, gtg_diag, dm_sum, dm, &o);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  if (iters) *iters = o.iters;
+  if (rnorm) *rnorm = o.rnorm;
+  if (bnorm) *bnorm = o.bnorm;
+  if (test2) *test2 = o.test2;
+  return FMT2D_OK;
+}
+
+int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (ms) *ms = ctx->lsqr->last_ms();
+  if (launches) *launches = ctx->lsqr->last_launches();
   return FMT2D_OK;
 }
 

@@ -1,0 +1,656 @@
+// Device LSQR (src/inversion2d.f90:6578-7167, smooth_type 1) and the G / G^T
+// products (src/inversion2d.f90:2997-3042).
+//
+// One LSQR iteration is two kernels:
+//   k_ls_fwd : u <- [G v; w_s L v; w_d v] - alpha u      (warp per CSR row for
+//              the data rows, thread per parameter for the smoothing and damping
+//              rows) and the pending w / dm update of the previous iteration;
+//   k_ls_adj : v <- [G^T u_G + w_s L u_L + w_d u_D] - beta v   (warp per CSC
+//              column), masked, plus the scalar recurrences of the rotation.
+// u and v are stored unnormalised together with their norms (beta, alpha):
+// readers divide on load, which removes the two normalisation passes of the
+// reference.  Every norm is a deterministic reduction: per-block partials
+// summed in a fixed order by the last block to finish (no spin-waits).  The
+// iteration loop runs as a captured CUDA graph of kIterPerGraph iterations;
+// after convergence the kernels return at their first instruction.
+#include "lsqr.h"
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <algorithm>
+#include <cmath>
+
+namespace fmt2d {
+
+#define LCK(x)                                                                \
+  do {                                                                        \
+    cudaError_t e_ = (x);                                                     \
+    if (e_ != cudaSuccess) return std::string(#x ": ") + cudaGetErrorString(e_); \
+  } while (0)
+
+namespace {
+
+constexpr int kIterPerGraph = 8;
+constexpr double kAtol = 1.0e-4;   // inversion2d.f90:6868
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Sum over the block; the result is valid in thread 0.
+__device__ double block_sum(double x) {
+  __shared__ double sh[32];
+  x = warp_sum(x);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    x = l < (int)(blockDim.x >> 5) ? sh[l] : 0.0;
+    x = warp_sum(x);
+  }
+  __syncthreads();
+  return x;
+}
+
+// Publishes this block's partial sum; in the last block to finish returns
+// true (in every thread) with the grid total in *total (thread 0 only).
+__device__ bool last_block_total(const LsqrDev& d, double partial, double* total) {
+  __shared__ bool last;
+  partial = block_sum(partial);
+  if (threadIdx.x == 0) {
+    d.part[blockIdx.x] = partial;
+    __threadfence();
+    const unsigned t = atomicAdd(&d.sc->count, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double s = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(d.part + i);
+  s = block_sum(s);
+  if (threadIdx.x == 0) {
+    *total = s;
+    d.sc->count = 0u;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool masked(const LsqrDev& d, int j) { return j < d.nvp && d.mask[j]; }
+__device__ __forceinline__ double w_smooth(const LsqrDev& d, int j) {
+  return j < d.nvp ? (d.mask[j] ? 0.0 : d.ws_v) : d.ws_i;
+}
+__device__ __forceinline__ double w_damp(const LsqrDev& d, int j) {
+  return j < d.nvp ? (d.mask[j] ? 0.0 : d.wd_v) : d.wd_i;
+}
+
+// apply_laplacian_smooth_2d (inversion2d.f90:1161-1249) at parameter j of the
+// vector x (stride-free accessor): 5-point Laplacian over the existing
+// neighbours of a velocity node (left, right, up, down, then -k centre), the
+// 1-D interface Laplacian with one-sided ends.
+__device__ __forceinline__ double lap_at(const LsqrDev& d, const double* x, int j) {
+  if (j < d.nvp) {
+    const int4 n = d.nb[j];
+    double acc = 0.0;
+    int k = 0;
+    if (n.x >= 0) { acc += x[n.x]; ++k; }
+    if (n.y >= 0) { acc += x[n.y]; ++k; }
+    if (n.z >= 0) { acc += x[n.z]; ++k; }
+    if (n.w >= 0) { acc += x[n.w]; ++k; }
+    return acc - (double)k * x[j];
+  }
+  const int ix = j - d.if_start + 1;   // 1-based node of the interface
+  if (ix < 1 || ix > d.if_n) return 0.0;
+  if (ix == 1) return (j + 1 < d.np) ? (0.0 + x[j + 1]) - x[j] : 0.0;
+  if (ix == d.if_n) return (0.0 + x[j - 1]) - x[j];
+  return ((0.0 + x[j - 1]) + x[j + 1]) - 2.0 * x[j];
+}
+
+// sum_k val[k] * x[idx[k]] over [k0, k1), lanes strided, warp-reduced.
+__device__ __forceinline__ double warp_dot(const int* __restrict__ idx,
+                                           const double* __restrict__ val, int k0, int k1,
+                                           const double* __restrict__ x, int lim) {
+  const int lane = threadIdx.x & 31;
+  double a0 = 0.0, a1 = 0.0;
+  int k = k0 + lane;
+  for (; k + 32 < k1; k += 64) {
+    const int j0 = __ldg(idx + k), j1 = __ldg(idx + k + 32);
+    const double g0 = __ldg(val + k), g1 = __ldg(val + k + 32);
+    if (j0 < lim) a0 += g0 * x[j0];
+    if (j1 < lim) a1 += g1 * x[j1];
+  }
+  if (k < k1) {
+    const int j0 = __ldg(idx + k);
+    if (j0 < lim) a0 += __ldg(val + k) * x[j0];
+  }
+  return warp_sum(a0 + a1);
+}
+
+__global__ void __launch_bounds__(kLsThreads) k_ls_init_u(LsqrDev d) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  double ss = 0.0;
+  for (int i = tid; i < d.nd; i += nth) {
+    const double r = d.residual[i];
+    d.u[i] = r;
+    ss += r * r;
+  }
+  for (int j = tid; j < d.np; j += nth) {
+    const double s = -(w_smooth(d, j) * lap_at(d, d.dm_sum, j));
+    const double t = -(w_damp(d, j) * d.dm_sum[j]);
+    d.u[d.nd + j] = s;
+    d.u[d.nd + d.np + j] = t;
+    ss += s * s + t * t;
+  }
+  double tot = 0.0;
+  if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
+    LsqrScalars& S = *d.sc;
+    const double bnorm = sqrt(tot);
+    S.bnorm = bnorm;
+    S.beta = bnorm;
+    S.alpha = 1.0;
+    S.iter = 0;
+    S.pending = kPendNone;
+    if (bnorm < 1.0e-30) {   // inversion2d.f90:6739-6745
+      S.state = kLsDone;
+      S.iters_out = 0;
+      S.rnorm = 0.0;
+      S.test2 = 0.0;
+    } else {
+      S.state = kLsInit;
+    }
+  }
+}
+
+// v <- A^T u (- beta v), masked; then the rotation of one LSQR step.
+__global__ void __launch_bounds__(kLsThreads) k_ls_adj(LsqrDev d) {
+  const int state = d.sc->state;
+  if (state != kLsInit && state != kLsRun) return;
+  const bool init = state == kLsInit;
+  const double beta = d.sc->beta, alpha = d.sc->alpha;
+  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  const double* uL = d.u + d.nd;
+  const double* uD = d.u + d.nd + d.np;
+  double ss = 0.0;
+  for (int j = warp; j < d.np; j += nwarp) {
+    const double g = warp_dot(d.crow, d.cval, d.cp[j], d.cp[j + 1], d.u, d.nd);
+    if (lane == 0) {
+      double atu = g / bsc;
+      atu = atu + (w_smooth(d, j) * lap_at(d, uL, j)) / bsc;
+      atu = atu + (w_damp(d, j) * uD[j]) / bsc;
+      double vn = init ? atu : atu - beta * (d.v[j] / asc);
+      if (masked(d, j)) vn = 0.0;
+      d.v[j] = vn;
+      ss += vn * vn;
+    }
+  }
+  double tot = 0.0;
+  if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
+    LsqrScalars& S = *d.sc;
+    const double a = sqrt(tot);
+    if (init) {
+      if (a < 1.0e-30) {   // inversion2d.f90:6853-6860
+        S.state = kLsDone;
+        S.iters_out = 0;
+        S.rnorm = S.bnorm;
+        S.test2 = 0.0;
+        return;
+      }
+      S.alpha = a;
+      S.phibar = S.beta;
+      S.rhobar = a;
+      S.anorm2 = a * a + S.beta * S.beta;
+      S.pending = kPendInitW;
+      S.state = kLsRun;
+      S.iter = 0;
+      return;
+    }
+    // inversion2d.f90:7122-7157
+    const double b = S.beta;
+    S.alpha = a;
+    S.anorm2 = S.anorm2 + a * a + b * b;
+    const double rho = sqrt(S.rhobar * S.rhobar + b * b);
+    const double c = S.rhobar / rho, s = b / rho;
+    const double theta = s * a;
+    S.rhobar = -c * a;
+    const double phi = c * S.phibar;
+    S.phibar = s * S.phibar;
+    S.t_r = theta / rho;
+    S.p_r = phi / rho;
+    S.pending = kPendUpdate;
+    S.rnorm = fabs(S.phibar);
+    const double arnorm = S.phibar * a * fabs(c);
+    S.test2 = arnorm / (sqrt(S.anorm2) * S.rnorm + 1.0e-30);
+    S.iter += 1;
+    if (S.test2 < kAtol || 1.0 + S.test2 <= 1.0) {
+      S.state = kLsFinal;
+      S.iters_out = S.iter;
+    } else if (S.iter >= d.max_iter) {
+      S.state = kLsFinal;
+      S.iters_out = d.max_iter + 1;   // a Fortran DO index after the last trip
+    }
+  }
+}
+
+// u <- A v - alpha u, and the pending w / dm update of the previous step.
+__global__ void __launch_bounds__(kLsThreads) k_ls_fwd(LsqrDev d) {
+  const int state = d.sc->state;
+  if (state != kLsRun && state != kLsFinal) return;
+  const bool run = state == kLsRun;
+  const int pending = d.sc->pending;
+  const double alpha = d.sc->alpha, beta = d.sc->beta;
+  const double t_r = d.sc->t_r, p_r = d.sc->p_r;
+  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
+  const int lane = threadIdx.x & 31;
+  double ss = 0.0;
+  if (run) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < d.nd; i += nwarp) {
+      const double g = warp_dot(d.col, d.val, d.rp[i], d.rp[i + 1], d.v, d.np);
+      if (lane == 0) {
+        const double un = g / asc - alpha * (d.u[i] / bsc);
+        d.u[i] = un;
+        ss += un * un;
+      }
+    }
+  }
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  double* uL = d.u + d.nd;
+  double* uD = d.u + d.nd + d.np;
+  for (int j = tid; j < d.np; j += nth) {
+    const double vn = d.v[j] / asc;
+    if (run) {
+      const double s = (w_smooth(d, j) * lap_at(d, d.v, j)) / asc - alpha * (uL[j] / bsc);
+      const double t = w_damp(d, j) * vn - alpha * (uD[j] / bsc);
+      uL[j] = s;
+      uD[j] = t;
+      ss += s * s + t * t;
+    }
+    if (pending == kPendInitW) {
+      d.w[j] = vn;
+    } else if (pending == kPendUpdate) {
+      const bool m = masked(d, j);
+      const double wo = d.w[j];
+      const double z = m ? 0.0 : wo;
+      double wn = vn - t_r * wo;
+      if (m) wn = 0.0;
+      d.w[j] = wn;
+      d.dm[j] = d.dm[j] + p_r * z;
+    }
+  }
+  double tot = 0.0;
+  if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
+    LsqrScalars& S = *d.sc;
+    if (run) S.beta = sqrt(tot);
+    S.pending = kPendNone;
+    if (state == kLsFinal) S.state = kLsDone;
+  }
+}
+
+__global__ void k_spmv_rows(LsqrDev d, const double* __restrict__ x, double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < d.nd; i += nwarp) {
+    const double g = warp_dot(d.col, d.val, d.rp[i], d.rp[i + 1], x, d.np);
+    if (lane == 0) y[i] = g;
+  }
+}
+
+__global__ void k_spmv_cols(LsqrDev d, const double* __restrict__ x, double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int j = warp; j < d.np; j += nwarp) {
+    const double g = warp_dot(d.crow, d.cval, d.cp[j], d.cp[j + 1], x, d.nd);
+    if (lane == 0) y[j] = g;
+  }
+}
+
+// Column sums of squares (inversion2d.f90:466-475).
+__global__ void k_gtg(LsqrDev d, double* out) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int j = warp; j < d.np; j += nwarp) {
+    double a = 0.0;
+    for (int k = d.cp[j] + lane; k < d.cp[j + 1]; k += 32) {
+      const double g = d.cval[k];
+      a += g * g;
+    }
+    a = warp_sum(a);
+    if (lane == 0) out[j] = a;
+  }
+}
+
+__global__ void k_mask(LsqrDev d, const double* gtg, double thr, uint8_t* mask) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int j = tid; j < d.np; j += nth) mask[j] = (j < d.nvp && gtg[j] < thr) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- CSR / CSC build
+__global__ void k_csr_rebase(int* rp, int nrp, int* col, long long nnz, int base, int np) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (long long k = tid; k < nrp; k += nth) rp[k] -= base;
+  for (long long k = tid; k < nnz; k += nth) {
+    const int c = col[k] - base;
+    col[k] = (c >= 0 && c < np) ? c : np;   // out of range: skipped (sparse_Ax/ATx)
+  }
+}
+
+__global__ void k_row_of(const int* rp, int nd, int* row_of, int* iota) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < nd; i += nwarp)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
+      row_of[k] = i;
+      iota[k] = k;
+    }
+}
+
+__global__ void k_count_cols(const int* col, long long nnz, int np, int* cnt) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (long long k = tid; k < nnz; k += nth)
+    if (col[k] < np) atomicAdd(cnt + col[k], 1);
+}
+
+__global__ void k_csc_fill(const int* perm, const int* row_of, const double* val, int nvalid,
+                           int* crow, double* cval) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int k = tid; k < nvalid; k += nth) {
+    const int p = perm[k];
+    crow[k] = row_of[p];
+    cval[k] = val[p];
+  }
+}
+
+}  // namespace
+
+void lsqr_launch_init_u(const LsqrDev& d, int grid, cudaStream_t st) {
+  k_ls_init_u<<<grid, kLsThreads, 0, st>>>(d);
+}
+void lsqr_launch_adj(const LsqrDev& d, int grid, cudaStream_t st) {
+  k_ls_adj<<<grid, kLsThreads, 0, st>>>(d);
+}
+void lsqr_launch_fwd(const LsqrDev& d, int grid, cudaStream_t st) {
+  k_ls_fwd<<<grid, kLsThreads, 0, st>>>(d);
+}
+void lsqr_launch_spmv(const LsqrDev& d, int transpose, const double* x, double* y, int grid,
+                      cudaStream_t st) {
+  if (transpose) k_spmv_cols<<<grid, kLsThreads, 0, st>>>(d, x, y);
+  else k_spmv_rows<<<grid, kLsThreads, 0, st>>>(d, x, y);
+}
+void lsqr_launch_gtg(const LsqrDev& d, double* out, int grid, cudaStream_t st) {
+  k_gtg<<<grid, kLsThreads, 0, st>>>(d, out);
+}
+void lsqr_launch_mask(const LsqrDev& d, const double* gtg, double thr, uint8_t* mask, int grid,
+                      cudaStream_t st) {
+  k_mask<<<grid, kLsThreads, 0, st>>>(d, gtg, thr, mask);
+}
+
+// ---------------------------------------------------------------- host
+Lsqr::Lsqr(int device, cudaStream_t st) : device_(device), st_(st) {
+  cudaSetDevice(device_);
+  int nsm = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ls_adj, kLsThreads, 0);
+  grid_ = std::max(1, nsm) * std::max(1, std::min(per_sm, 8));
+  cudaMallocHost(&h_sc_, sizeof(LsqrScalars));
+}
+
+Lsqr::~Lsqr() {
+  cudaSetDevice(device_);
+  if (h_sc_) cudaFreeHost(h_sc_);
+}
+
+std::string Lsqr::set_geometry(const Model& m) {
+  const int nx = m.nx, nz = m.nz;
+  nvp_ = m.n_vel_parms;
+  if_start_ = m.n_vel_parms;
+  if_n_ = m.iface_inv > 0 ? nx : 0;
+  std::vector<int4> nb((size_t)std::max(nvp_, 1), make_int4(-1, -1, -1, -1));
+  auto id = [&](int ix, int iz) { return m.inv_idx[(size_t)iz * nx + ix]; };
+  for (int iz = 0; iz < nz; ++iz)
+    for (int ix = 0; ix < nx; ++ix) {
+      const int k = id(ix, iz);
+      if (k <= 0) continue;
+      int4 n = make_int4(-1, -1, -1, -1);
+      if (ix > 0 && id(ix - 1, iz) > 0) n.x = id(ix - 1, iz) - 1;
+      if (ix < nx - 1 && id(ix + 1, iz) > 0) n.y = id(ix + 1, iz) - 1;
+      if (iz > 0 && id(ix, iz - 1) > 0) n.z = id(ix, iz - 1) - 1;
+      if (iz < nz - 1 && id(ix, iz + 1) > 0) n.w = id(ix, iz + 1) - 1;
+      nb[k - 1] = n;
+    }
+  cudaSetDevice(device_);
+  nb_.alloc(nb.size() * sizeof(int4));
+  if (!nb_.p) return "device allocation failed (Laplacian table)";
+  LCK(cudaMemcpyAsync(nb_.p, nb.data(), nb.size() * sizeof(int4), cudaMemcpyHostToDevice, st_));
+  LCK(cudaStreamSynchronize(st_));
+  have_geom_ = true;
+  return std::string();
+}
+
+LsqrDev Lsqr::view() const {
+  LsqrDev d;
+  d.nd = nd_;
+  d.np = np_;
+  d.nvp = std::min(nvp_, np_);
+  d.rp = rp_.as<int>();
+  d.col = col_.as<int>();
+  d.val = val_.as<double>();
+  d.cp = cp_.as<int>();
+  d.crow = crow_.as<int>();
+  d.cval = cval_.as<double>();
+  d.nb = nb_.as<int4>();
+  d.if_start = if_start_;
+  d.if_n = if_n_;
+  d.mask = mask_.as<uint8_t>();
+  d.residual = res_.as<double>();
+  d.dm_sum = dms_.as<double>();
+  d.u = u_.as<double>();
+  d.v = v_.as<double>();
+  d.w = w_.as<double>();
+  d.dm = dm_.as<double>();
+  d.part = part_.as<double>();
+  d.sc = sc_.as<LsqrScalars>();
+  return d;
+}
+
+std::string Lsqr::set_matrix(int ndata, int nparm, const int* row_ptr, const int* col,
+                             const double* val, int base) {
+  if (ndata < 0 || nparm <= 0 || !row_ptr || (base != 0 && base != 1))
+    return "bad matrix dimensions";
+  const long long nnz = (long long)row_ptr[ndata] - base;
+  if (row_ptr[0] != base || nnz < 0 || nnz > 0x7fffffffLL) return "bad row pointer";
+  for (int i = 0; i < ndata; ++i)
+    if (row_ptr[i + 1] < row_ptr[i]) return "row pointer not monotone";
+  if (nnz > 0 && (!col || !val)) return "null column or value array";
+  cudaSetDevice(device_);
+  nd_ = ndata;
+  np_ = nparm;
+  nnz_ = nnz;
+  rp_.alloc((size_t)(ndata + 1) * 4);
+  col_.alloc((size_t)nnz * 4);
+  val_.alloc((size_t)nnz * 8);
+  if (!rp_.p || !col_.p || !val_.p) return "device allocation failed (CSR)";
+  LCK(cudaMemcpyAsync(rp_.p, row_ptr, (size_t)(ndata + 1) * 4, cudaMemcpyHostToDevice, st_));
+  if (nnz) {
+    LCK(cudaMemcpyAsync(col_.p, col, (size_t)nnz * 4, cudaMemcpyHostToDevice, st_));
+    LCK(cudaMemcpyAsync(val_.p, val, (size_t)nnz * 8, cudaMemcpyHostToDevice, st_));
+  }
+  k_csr_rebase<<<grid_, kLsThreads, 0, st_>>>(rp_.as<int>(), ndata + 1, col_.as<int>(), nnz, base,
+                                              nparm);
+  LCK(cudaGetLastError());
+  return build_csc();
+}
+
+std::string Lsqr::build_csc() {
+  const int nnz = (int)nnz_;
+  cp_.alloc((size_t)(np_ + 1) * 4);
+  crow_.alloc((size_t)nnz * 4);
+  cval_.alloc((size_t)nnz * 8);
+  part_.alloc((size_t)grid_ * 8);
+  sc_.alloc(sizeof(LsqrScalars));
+  if (!cp_.p || !crow_.p || !cval_.p || !part_.p || !sc_.p) return "device allocation failed (CSC)";
+  DevBuf row_of, iota, keys, perm, cnt, tmp;
+  row_of.alloc((size_t)nnz * 4);
+  iota.alloc((size_t)nnz * 4);
+  keys.alloc((size_t)nnz * 4);
+  perm.alloc((size_t)nnz * 4);
+  cnt.alloc((size_t)(np_ + 1) * 4);
+  if (!row_of.p || !iota.p || !keys.p || !perm.p || !cnt.p) return "device allocation failed (CSC build)";
+  LCK(cudaMemsetAsync(cnt.p, 0, (size_t)(np_ + 1) * 4, st_));
+  k_row_of<<<grid_, kLsThreads, 0, st_>>>(rp_.as<int>(), nd_, row_of.as<int>(), iota.as<int>());
+  k_count_cols<<<grid_, kLsThreads, 0, st_>>>(col_.as<int>(), nnz, np_, cnt.as<int>());
+  LCK(cudaGetLastError());
+  int end_bit = 1;
+  while (end_bit < 31 && (1LL << end_bit) <= np_) ++end_bit;
+  size_t sort_bytes = 0, scan_bytes = 0;
+  LCK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, col_.as<int>(), keys.as<int>(),
+                                      iota.as<int>(), perm.as<int>(), nnz, 0, end_bit, st_));
+  LCK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt.as<int>(), cp_.as<int>(), np_ + 1,
+                                    st_));
+  tmp.alloc(std::max(sort_bytes, scan_bytes));
+  if (!tmp.p) return "device allocation failed (sort workspace)";
+  if (nnz)
+    LCK(cub::DeviceRadixSort::SortPairs(tmp.p, sort_bytes, col_.as<int>(), keys.as<int>(),
+                                        iota.as<int>(), perm.as<int>(), nnz, 0, end_bit, st_));
+  LCK(cub::DeviceScan::ExclusiveSum(tmp.p, scan_bytes, cnt.as<int>(), cp_.as<int>(), np_ + 1, st_));
+  int nvalid = 0;
+  LCK(cudaMemcpyAsync(&nvalid, cp_.as<int>() + np_, 4, cudaMemcpyDeviceToHost, st_));
+  LCK(cudaStreamSynchronize(st_));
+  if (nvalid > 0)
+    k_csc_fill<<<grid_, kLsThreads, 0, st_>>>(perm.as<int>(), row_of.as<int>(), val_.as<double>(),
+                                              nvalid, crow_.as<int>(), cval_.as<double>());
+  LCK(cudaGetLastError());
+  LCK(cudaStreamSynchronize(st_));
+  return std::string();
+}
+
+std::string Lsqr::spmv(int transpose, const double* x, double* y) {
+  if (!rp_.p) return "no matrix set";
+  cudaSetDevice(device_);
+  const int nin = transpose ? nd_ : np_, nout = transpose ? np_ : nd_;
+  x_.alloc((size_t)std::max(nin, 1) * 8);
+  y_.alloc((size_t)std::max(nout, 1) * 8);
+  if (!x_.p || !y_.p) return "device allocation failed";
+  if (nin) LCK(cudaMemcpyAsync(x_.p, x, (size_t)nin * 8, cudaMemcpyHostToDevice, st_));
+  lsqr_launch_spmv(view(), transpose, x_.as<double>(), y_.as<double>(), grid_, st_);
+  LCK(cudaGetLastError());
+  if (nout) LCK(cudaMemcpyAsync(y, y_.p, (size_t)nout * 8, cudaMemcpyDeviceToHost, st_));
+  LCK(cudaStreamSynchronize(st_));
+  return std::string();
+}
+
+std::string Lsqr::gtg_diag(double* out) {
+  if (!rp_.p) return "no matrix set";
+  cudaSetDevice(device_);
+  y_.alloc((size_t)np_ * 8);
+  if (!y_.p) return "device allocation failed";
+  lsqr_launch_gtg(view(), y_.as<double>(), grid_, st_);
+  LCK(cudaGetLastError());
+  LCK(cudaMemcpyAsync(out, y_.p, (size_t)np_ * 8, cudaMemcpyDeviceToHost, st_));
+  LCK(cudaStreamSynchronize(st_));
+  return std::string();
+}
+
+std::string Lsqr::solve(const LsqrParams& p, const double* residual, const double* gtg,
+                        const double* dm_sum, double* dm, LsqrOut* out) {
+  if (!rp_.p) return "no matrix set";
+  if (!have_geom_) return "no model geometry for the smoothing operator";
+  if (p.smooth_type != 1) return "smooth_type must be 1 (Laplacian)";
+  if (p.max_iter < 1) return "max_iter must be >= 1";
+  if (np_ != if_start_ + if_n_) return "matrix columns differ from the model's inversion parameters";
+  if (!dm) return "null output";
+  cudaSetDevice(device_);
+  const size_t na = (size_t)nd_ + 2 * (size_t)np_;
+  res_.alloc((size_t)std::max(nd_, 1) * 8);
+  dms_.alloc((size_t)np_ * 8);
+  gtg_.alloc((size_t)np_ * 8);
+  mask_.alloc((size_t)np_);
+  u_.alloc(na * 8);
+  v_.alloc((size_t)np_ * 8);
+  w_.alloc((size_t)np_ * 8);
+  dm_.alloc((size_t)np_ * 8);
+  if (!res_.p || !dms_.p || !gtg_.p || !mask_.p || !u_.p || !v_.p || !w_.p || !dm_.p)
+    return "device allocation failed (LSQR vectors)";
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st_);
+  if (nd_) {
+    if (!residual) return "null residual";
+    LCK(cudaMemcpyAsync(res_.p, residual, (size_t)nd_ * 8, cudaMemcpyHostToDevice, st_));
+  }
+  if (dm_sum) LCK(cudaMemcpyAsync(dms_.p, dm_sum, (size_t)np_ * 8, cudaMemcpyHostToDevice, st_));
+  else LCK(cudaMemsetAsync(dms_.p, 0, (size_t)np_ * 8, st_));
+  LsqrDev d = view();
+  d.ws_v = p.w_smooth;
+  d.ws_i = p.w_smooth_iface;
+  d.wd_v = p.wdv;
+  d.wd_i = p.wdv_iface;
+  d.max_iter = p.max_iter;
+  int launches = 0;
+  if (gtg) {
+    LCK(cudaMemcpyAsync(gtg_.p, gtg, (size_t)np_ * 8, cudaMemcpyHostToDevice, st_));
+  } else {
+    lsqr_launch_gtg(d, gtg_.as<double>(), grid_, st_);
+    ++launches;
+  }
+  lsqr_launch_mask(d, gtg_.as<double>(), p.eps_min * 0.01, mask_.as<uint8_t>(), grid_, st_);
+  LCK(cudaMemsetAsync(dm_.p, 0, (size_t)np_ * 8, st_));
+  LCK(cudaMemsetAsync(sc_.p, 0, sizeof(LsqrScalars), st_));
+  lsqr_launch_init_u(d, grid_, st_);
+  lsqr_launch_adj(d, grid_, st_);
+  lsqr_launch_fwd(d, grid_, st_);
+  launches += 4;
+  LCK(cudaGetLastError());
+  // the iteration loop: a graph of kIterPerGraph (adj, fwd) pairs
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  LCK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < kIterPerGraph; ++k) {
+    lsqr_launch_adj(d, grid_, st_);
+    lsqr_launch_fwd(d, grid_, st_);
+  }
+  LCK(cudaStreamEndCapture(st_, &graph));
+  LCK(cudaGraphInstantiate(&exec, graph, 0));
+  const int max_graphs = p.max_iter / kIterPerGraph + 2;
+  std::string err;
+  for (int gi = 0; gi <= max_graphs; ++gi) {
+    LCK(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(LsqrScalars), cudaMemcpyDeviceToHost, st_));
+    LCK(cudaStreamSynchronize(st_));
+    if (h_sc_->state == kLsDone) break;
+    if (gi == max_graphs) { err = "LSQR did not terminate"; break; }
+    LCK(cudaGraphLaunch(exec, st_));
+    launches += 2 * kIterPerGraph;
+  }
+  cudaEventRecord(e1, st_);
+  LCK(cudaMemcpyAsync(dm, dm_.p, (size_t)np_ * 8, cudaMemcpyDeviceToHost, st_));
+  LCK(cudaStreamSynchronize(st_));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  last_ms_ = ms;
+  last_launches_ = launches;
+  if (!err.empty()) return err;
+  if (out) {
+    out->iters = h_sc_->iters_out;
+    out->rnorm = h_sc_->rnorm;
+    out->bnorm = h_sc_->bnorm;
+    out->test2 = h_sc_->test2;
+  }
+  return std::string();
+}
+
+}  // namespace fmt2d

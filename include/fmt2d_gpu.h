@@ -19,6 +19,12 @@
  *                           src/mod_fmt2d.f90:706-712) for every source
  *   fmt2d_get_field      <- reading tf%arrivaltime / tf%time_gradient
  *                           (src/mod_fmt2d.f90:262-279) in region node order
+ *   fmt2d_set_frechet    <- the CSR that read_frechet_data2d builds
+ *                           (src/inversion2d.f90:3965-4052) after the column
+ *                           and row scaling of src/inversion2d.f90:371-379
+ *   fmt2d_spmv           <- sparse_Ax / sparse_ATx (src/inversion2d.f90:2997-3042)
+ *   fmt2d_gtg_diag       <- the gtg_diag loop of src/inversion2d.f90:466-475
+ *   fmt2d_lsqr           <- run_lsqr (src/inversion2d.f90:6578-7167)
  *
  * Conventions: every function returns 0 on success and a negative FMT2D_ERR_*
  * code on failure (never exits the process); fmt2d_last_error() returns the
@@ -99,6 +105,40 @@ FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double
  * Writes min(n, FMT2D_N_STATS) values.  No reference counterpart (diagnostics). */
 #define FMT2D_N_STATS 11
 FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
+
+/* Sensitivity matrix G (ndata picks x nparm parameters) as CSR host arrays,
+ * index_base 1 for the reference's 1-based gindx / row_ptr (row_ptr has
+ * ndata+1 entries).  Columns outside 1..nparm are kept but skipped by every
+ * product, like sparse_Ax / sparse_ATx.  The context keeps G on the device as
+ * CSR and as CSC (columns in ascending row order) until the next call. */
+FMT2D_API int fmt2d_set_frechet(fmt2d_ctx* ctx, int ndata, int nparm, const int* row_ptr,
+                                const int* gindx, const double* gval, int index_base);
+/* y = G x (transpose 0: x[nparm] -> y[ndata]) or y = G^T x (transpose 1). */
+FMT2D_API int fmt2d_spmv(fmt2d_ctx* ctx, int transpose, const double* x, double* y);
+/* gtg[j] = sum over rows of G(i,j)^2, j = 1..nparm. */
+FMT2D_API int fmt2d_gtg_diag(fmt2d_ctx* ctx, double* gtg);
+
+/* run_lsqr's arguments that are not arrays.  smooth_type 1 (Laplacian) is the
+ * augmented system [G; w_s L; w_d I] with the model's inversion numbering;
+ * max_iter is the reference's min(lsqr_max_iter, 2000), >= 1. */
+typedef struct fmt2d_lsqr_params {
+  int smooth_type;
+  int max_iter;
+  double wdv, wdv_iface;            /* damping weights (velocity, interface) */
+  double w_smooth, w_smooth_iface;  /* smoothing weights */
+  double eps_min;                   /* velocity columns with gtg < 0.01 eps_min are masked */
+} fmt2d_lsqr_params;
+
+/* LSQR on the current G: residual[ndata], gtg_diag[nparm] (NULL: computed
+ * from G), dm_sum[nparm] (NULL: zeros) -> dm[nparm] and the reference's
+ * lsqr_iter_out, rnorm_out, bnorm_out, test2_out (any may be NULL).  Needs an
+ * uploaded model whose n_inv_parms equals nparm. */
+FMT2D_API int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params, const double* residual,
+                         const double* gtg_diag, const double* dm_sum, double* dm, int* iters,
+                         double* rnorm, double* bnorm, double* test2);
+/* Device milliseconds and kernel launches of the last fmt2d_lsqr (diagnostics,
+ * no reference counterpart). */
+FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* The CUDA stream (cudaStream_t) all work of the context is issued on, for
  * callers that record events around fmt2d_forward.  No reference counterpart. */

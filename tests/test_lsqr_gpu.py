@@ -1,0 +1,137 @@
+"""Device G products and LSQR (fmt2d_spmv / fmt2d_gtg_diag / fmt2d_lsqr)
+against the oracle's restatement of sparse_Ax / sparse_ATx and run_lsqr
+(src/inversion2d.f90:2997-3042, 6578-7167).
+
+Tolerances: products and gtg within 1e-12 relative (FP64, different
+summation order).  LSQR iterates within 1e-6 of max|dm| at fixed iteration
+counts up to 40 (both paths amplify rounding differences by about 1.3x per
+iteration, so iterates are compared where that growth is still small); runs
+to convergence must stop at the same iteration (+-2) with the misfit of the
+augmented system within 1e-4 relative and dm within 1e-4 relative when the
+solve converges within 60 iterations.
+"""
+import numpy as np
+import pytest
+
+from fmt2d_b200 import synth
+from _cases import oracle_G, random_G, csr_to_scipy, ref_ops
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small(oracle_lib):
+    from fmt2d_b200.api import Fmt2d
+    m = synth.small_model()
+    o = oracle_lib.Oracle(m)
+    nd, npar, rp, gi, gv, tc, used = oracle_G(o, m)
+    g = Fmt2d(0).upload(m)
+    g.set_frechet(nd, npar, rp, gi, gv)
+    inv, nvp, _ = o.inv_idx()
+    return m, o, g, nd, npar, nvp, rp, gi, gv
+
+
+def _inputs(nd, npar, rp, gi, gv, seed=11):
+    G = csr_to_scipy(nd, npar, rp, gi, gv)
+    rng = np.random.default_rng(seed)
+    r = rng.normal(0.0, 0.05, nd)
+    dm_sum = rng.normal(0.0, 0.01, npar)
+    gtg = np.asarray(G.multiply(G).sum(axis=0)).ravel()
+    eps_min = max(1e-6, 1e-4 * gtg.max())
+    return G, r, dm_sum, gtg, eps_min
+
+
+def test_products_and_gtg(oracle_lib, small):
+    m, o, g, nd, npar, nvp, rp, gi, gv = small
+    rng = np.random.default_rng(5)
+    x, y = rng.normal(size=npar), rng.normal(size=nd)
+    for tr, inp in ((False, x), (True, y)):
+        ref = oracle_lib.spmv(nd, npar, gi, gv, rp, inp, transpose=tr)
+        out = g.spmv(inp, transpose=tr)
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+    G = csr_to_scipy(nd, npar, rp, gi, gv)
+    gtg = np.asarray(G.multiply(G).sum(axis=0)).ravel()
+    assert np.abs(g.gtg_diag() - gtg).max() <= 1e-12 * gtg.max()
+
+
+@pytest.mark.parametrize("ws_v,ws_i,wd_v,wd_i", [(0.0, 0.0, 1.0, 1.0), (3.0, 3.0, 0.5, 0.5),
+                                                 (10.0, 2.0, 1.0, 0.3)])
+@pytest.mark.parametrize("max_iter", [8, 40, 2000])
+def test_lsqr_against_oracle(oracle_lib, small, ws_v, ws_i, wd_v, wd_i, max_iter):
+    m, o, g, nd, npar, nvp, rp, gi, gv = small
+    G, r, dm_sum, gtg, eps_min = _inputs(nd, npar, rp, gi, gv)
+    dmo, ito, rno, t2o = o.lsqr(nd, npar, gi, gv, rp, r, gtg, dm_sum, eps_min, wd_v, wd_i, ws_v,
+                                ws_i, max_iter)
+    dmg, itg, rng_, bng, t2g = g.lsqr(r, dm_sum, gtg, wdv=wd_v, wdv_iface=wd_i, w_smooth=ws_v,
+                                      w_smooth_iface=ws_i, eps_min=eps_min, max_iter=max_iter)
+    scale = np.abs(dmo).max()
+    if max_iter <= 40:
+        assert itg == ito
+        assert np.abs(dmg - dmo).max() <= 1e-6 * scale
+        assert abs(rng_ - rno) <= 1e-9 * bng
+        return
+    assert abs(itg - ito) <= 2, (itg, ito)
+    mask = gtg[:nvp] < 0.01 * eps_min
+    A, ws, wd = ref_ops(o, G, nvp, mask, ws_v, ws_i, wd_v, wd_i)
+    b = np.concatenate([r, -(ws * o.laplacian(npar, dm_sum)), -(wd * dm_sum)])
+    mo, mg = np.linalg.norm(A @ dmo - b), np.linalg.norm(A @ dmg - b)
+    assert abs(mg - mo) <= 1e-4 * mo
+    assert abs(rng_ - mg) <= 1e-6 * np.linalg.norm(b)
+    if ito <= 60:
+        assert np.abs(dmg - dmo).max() <= 1e-4 * scale
+
+
+def test_lsqr_defaults_and_zero_rhs(oracle_lib, small):
+    """gtg computed on the device equals the host one; dm_sum NULL means
+    zeros; a zero right-hand side stops before the first iteration."""
+    m, o, g, nd, npar, nvp, rp, gi, gv = small
+    G, r, dm_sum, gtg, eps_min = _inputs(nd, npar, rp, gi, gv)
+    kw = dict(wdv=1.0, wdv_iface=1.0, w_smooth=2.0, w_smooth_iface=2.0, eps_min=eps_min,
+              max_iter=30)
+    a = g.lsqr(r, None, gtg, **kw)
+    b = g.lsqr(r, np.zeros(npar), None, **kw)
+    assert a[1] == b[1]
+    assert np.abs(a[0] - b[0]).max() <= 1e-12 * np.abs(a[0]).max()
+    z = g.lsqr(np.zeros(nd), np.zeros(npar), gtg, **kw)
+    assert z[1] == 0 and not z[0].any() and z[3] == 0.0
+
+
+def test_out_of_range_columns_and_empty_rows(oracle_lib, small):
+    """Columns outside 1..nparm are skipped and empty rows give zeros, as in
+    sparse_Ax / sparse_ATx."""
+    m, o, g0, nd, npar, nvp, rp, gi, gv = small
+    from fmt2d_b200.api import Fmt2d
+    gi2 = gi.copy()
+    gi2[::97] = npar + 3
+    gi2[5::101] = 0
+    rp2 = np.concatenate([rp[:10], rp[9:10], rp[10:]]).astype(np.int32)   # an empty row 9
+    nd2 = nd + 1
+    g = Fmt2d(0).upload(m)
+    g.set_frechet(nd2, npar, rp2, gi2, gv)
+    rng = np.random.default_rng(2)
+    x, y = rng.normal(size=npar), rng.normal(size=nd2)
+    for tr, inp in ((False, x), (True, y)):
+        ref = oracle_lib.spmv(nd2, npar, gi2, gv, rp2, inp, transpose=tr)
+        out = g.spmv(inp, transpose=tr)
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert g.spmv(x)[9] == 0.0
+
+
+def test_lsqr_larger_random(oracle_lib):
+    """A 401x121-grid model with 4000 ray-like random rows (about 0.8 M
+    entries) at a fixed iteration count."""
+    from fmt2d_b200.api import Fmt2d
+    m = synth.config(0)
+    o = oracle_lib.Oracle(m)
+    inv, nvp, npar = o.inv_idx()
+    nd, npar, rp, gi, gv = random_G(4000, npar, 200, seed=9)
+    G, r, dm_sum, gtg, eps_min = _inputs(nd, npar, rp, gi, gv, seed=4)
+    g = Fmt2d(0).upload(m)
+    g.set_frechet(nd, npar, rp, gi, gv)
+    dmo, ito, rno, _ = o.lsqr(nd, npar, gi, gv, rp, r, gtg, dm_sum, eps_min, 1.0, 1.0, 10.0, 10.0,
+                              25)
+    dmg, itg, rng_, bng, _ = g.lsqr(r, dm_sum, gtg, wdv=1.0, wdv_iface=1.0, w_smooth=10.0,
+                                    w_smooth_iface=10.0, eps_min=eps_min, max_iter=25)
+    assert itg == ito
+    assert np.abs(dmg - dmo).max() <= 1e-6 * np.abs(dmo).max()
+    assert abs(rng_ - rno) <= 1e-9 * bng
