@@ -3,7 +3,12 @@
  * the CPU-baseline leg of bench.py as the checker; the product library never
  * links it.  All arrays are caller-owned.  Grid arrays are nx*nz with ix
  * fastest; region node arrays are 0-based copies of the reference's 1-based
- * node numbering (entry k holds node id k+1). */
+ * node numbering (entry k holds node id k+1).
+ *
+ * Parity unpinned: the reference is Fortran and cannot be compiled here (no
+ * Fortran compiler), and it ships no tests or golden vectors.  The restatement
+ * is checked against closed-form traveltimes and against SciPy's LSQR instead
+ * (tests/test_oracle_kat.py, tests/test_lsqr_oracle.py). */
 #ifndef FMT2D_ORACLE_H
 #define FMT2D_ORACLE_H
 #include <stdint.h>

@@ -4,6 +4,9 @@
 // or calls this code; tests, the smoke check and the CPU-baseline leg of the
 // benchmark use it as the checker.
 //
+// Parity unpinned: the reference cannot be built here (no Fortran compiler)
+// and has no golden vectors; analytic known answers and SciPy's LSQR pin it.
+//
 // Indexing mirrors the reference on purpose, because node and parameter
 // numbering is a bit-exact contract: grid indices ix, iz and region node ids
 // are 1-based, 0 means "no node".  Every routine names the reference routine
