@@ -71,6 +71,9 @@ def lib():
     L.fmt2d_gtg_diag.argtypes = [V, C.c_void_p]
     L.fmt2d_lsqr.argtypes = [V, P(LsqrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              P(C.c_int), P(C.c_double), P(C.c_double), P(C.c_double)]
+    L.fmt2d_lsqr_noalloc.argtypes = [V, P(LsqrParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, P(C.c_int), P(C.c_double), P(C.c_double),
+                                     P(C.c_double)]
     L.fmt2d_lsqr_stats.argtypes = [V, P(C.c_double), P(C.c_int)]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int

@@ -221,6 +221,39 @@ int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residua
   return FMT2D_OK;
 }
 
+int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residual,
+                       const double* gtg_diag, const double* dm_sum, double* dm, int* iters,
+                       double* rnorm, double* bnorm, double* test2) {
+  if (!ctx || !p || !dm) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
+  if (p->smooth_type != 1) return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1 (Laplacian)");
+  if (p->max_iter < 1) return ctx->fail(FMT2D_ERR_ARG, "max_iter must be >= 1");
+  if (ctx->lsqr->nparm() != ctx->model.n_inv_parms)
+    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the model's inversion parameters");
+  fmt2d::LsqrParams q;
+  q.smooth_type = p->smooth_type;
+  q.max_iter = p->max_iter;
+  q.wdv = p->wdv;
+  q.wdv_iface = p->wdv_iface;
+  q.w_smooth = p->w_smooth;
+  q.w_smooth_iface = p->w_smooth_iface;
+  q.eps_min = p->eps_min;
+  fmt2d::LsqrOut o;
+  const std::string e = ctx->lsqr->solve_noalloc(q, residual, gtg_diag, dm_sum, dm, &o);
+  if (!e.empty())
+    return ctx->fail(e.find("too large") != std::string::npos ||
+                             e.find("null") != std::string::npos ? FMT2D_ERR_ARG : FMT2D_ERR_CUDA,
+                     e);
+  if (iters) *iters = o.iters;
+  if (rnorm) *rnorm = o.rnorm;
+  if (bnorm) *bnorm = o.bnorm;
+  if (test2) *test2 = o.test2;
+  return FMT2D_OK;
+}
+
 int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
   if (!ctx) return FMT2D_ERR_ARG;
   int code = 0;

@@ -18,6 +18,7 @@
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 namespace fmt2d {
 
@@ -649,6 +650,133 @@ std::string Lsqr::solve(const LsqrParams& p, const double* residual, const doubl
     out->rnorm = h_sc_->rnorm;
     out->bnorm = h_sc_->bnorm;
     out->test2 = h_sc_->test2;
+  }
+  return std::string();
+}
+
+
+// ---------------------------------------------------------------- no-alloc solve
+// LSQR for callers that cannot allocate device memory while they solve: a
+// driver that overlaps this solve with work on other streams (cudaMalloc and
+// cudaFree can synchronise the whole device and stall those streams), or a
+// host program whose device memory is all reserved up front by its own pool
+// allocator (a caching allocator or a Fortran driver's fixed arena), where a
+// new cudaMalloc fails or fragments that reserve.  The work vectors live in
+// one file-scope device array of kNoAllocBytes, which every GPU that loads
+// the library holds until the process exits.  Every call shares it, so calls
+// that overlap on the GPU (other host threads, other contexts of the same
+// device) race on it; each call clears what has to start at zero.
+namespace {
+
+constexpr size_t kNoAllocDoubles = size_t(1) << 22;   // 32 MiB
+constexpr size_t kNoAllocAlign = 32;                  // doubles (256 bytes)
+constexpr size_t kNoAllocPart = 2048;                 // per-block partial sums
+
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};
+
+// Device address of the scratch array on `device` (which must be current).
+// The first call on a device looks it up with cudaGetSymbolAddress: in host
+// code the array's name is only a host-side stand-in, so kernels must be
+// given this address.
+std::string noalloc_scratch(int device, double** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device < 0 || device >= 256) return "device ordinal out of range";
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e);
+    g_noalloc_ptr[device] = p;
+  }
+  *out = static_cast<double*>(g_noalloc_ptr[device]);
+  return std::string();
+}
+
+size_t round_up(size_t n) { return (n + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+
+}  // namespace
+
+std::string Lsqr::solve_noalloc(const LsqrParams& p, const double* residual, const double* gtg,
+                                const double* dm_sum, double* dm, LsqrOut* out) {
+  if (!rp_.p) return "no matrix set";
+  if (!have_geom_) return "no model geometry for the smoothing operator";
+  if (p.smooth_type != 1) return "smooth_type must be 1 (Laplacian)";
+  if (p.max_iter < 1) return "max_iter must be >= 1";
+  if (np_ != if_start_ + if_n_) return "matrix columns differ from the model's inversion parameters";
+  if (!dm || (nd_ > 0 && !residual)) return "null device vector";
+  if (grid_ > (int)kNoAllocPart) return "launch grid larger than the scratch partial-sum area";
+  // scratch layout (doubles): scalars | partials | u | v | w | gtg | zeros | mask bytes
+  const size_t o_sc = 0, o_part = kNoAllocAlign;
+  const size_t o_u = o_part + kNoAllocPart;
+  const size_t o_v = o_u + round_up((size_t)nd_ + 2 * (size_t)np_);
+  const size_t o_w = o_v + round_up(np_);
+  const size_t o_g = o_w + round_up(np_);
+  const size_t o_z = o_g + round_up(np_);
+  const size_t o_m = o_z + round_up(np_);
+  const size_t need = o_m + round_up(((size_t)np_ + 7) / 8);
+  if (need > kNoAllocDoubles)
+    return "problem too large for the no-alloc scratch: needs " + std::to_string(need * 8) +
+           " bytes (ndata + 6.125 nparm doubles plus 16.6 KB), the array holds " +
+           std::to_string(kNoAllocDoubles * 8) + " bytes";
+  cudaSetDevice(device_);
+  double* S = nullptr;
+  std::string e = noalloc_scratch(device_, &S);
+  if (!e.empty()) return e;
+  LsqrDev d = view();
+  d.sc = reinterpret_cast<LsqrScalars*>(S + o_sc);
+  d.part = S + o_part;
+  d.u = S + o_u;
+  d.v = S + o_v;
+  d.w = S + o_w;
+  d.dm = dm;
+  d.mask = reinterpret_cast<uint8_t*>(S + o_m);
+  d.residual = residual;
+  d.ws_v = p.w_smooth;
+  d.ws_i = p.w_smooth_iface;
+  d.wd_v = p.wdv;
+  d.wd_i = p.wdv_iface;
+  d.max_iter = p.max_iter;
+  if (!dm_sum) {
+    LCK(cudaMemsetAsync(S + o_z, 0, (size_t)np_ * 8, st_));
+    dm_sum = S + o_z;
+  }
+  d.dm_sum = dm_sum;
+  if (!gtg) {
+    lsqr_launch_gtg(d, S + o_g, grid_, st_);
+    gtg = S + o_g;
+  }
+  lsqr_launch_mask(d, gtg, p.eps_min * 0.01, reinterpret_cast<uint8_t*>(S + o_m), grid_, st_);
+  LCK(cudaMemsetAsync(dm, 0, (size_t)np_ * 8, st_));
+  LCK(cudaMemsetAsync(d.sc, 0, sizeof(LsqrScalars), st_));
+  lsqr_launch_init_u(d, grid_, st_);
+  lsqr_launch_adj(d, grid_, st_);
+  lsqr_launch_fwd(d, grid_, st_);
+  LCK(cudaGetLastError());
+  LsqrScalars hs;
+  const int max_rounds = p.max_iter / kIterPerGraph + 2;
+  for (int r = 0;; ++r) {
+    LCK(cudaMemcpyAsync(&hs, d.sc, sizeof(LsqrScalars), cudaMemcpyDeviceToHost, st_));
+    LCK(cudaStreamSynchronize(st_));
+    if (hs.state == kLsDone) break;
+    if (r == max_rounds) return "LSQR did not terminate";
+    for (int k = 0; k < kIterPerGraph; ++k) {
+      lsqr_launch_adj(d, grid_, st_);
+      lsqr_launch_fwd(d, grid_, st_);
+    }
+    LCK(cudaGetLastError());
+  }
+  if (out) {
+    out->iters = hs.iters_out;
+    out->rnorm = hs.rnorm;
+    out->bnorm = hs.bnorm;
+    out->test2 = hs.test2;
   }
   return std::string();
 }

@@ -92,6 +92,10 @@ class Lsqr {
   std::string gtg_diag(double* out);
   std::string solve(const LsqrParams& p, const double* residual, const double* gtg,
                     const double* dm_sum, double* dm, LsqrOut* out);
+  // The same solve with every work vector in a file-scope device array
+  // (nothing allocated); residual, gtg, dm_sum and dm are device pointers.
+  std::string solve_noalloc(const LsqrParams& p, const double* residual, const double* gtg,
+                            const double* dm_sum, double* dm, LsqrOut* out);
   int ndata() const { return nd_; }
   int nparm() const { return np_; }
   long long nnz() const { return nnz_; }

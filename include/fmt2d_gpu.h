@@ -136,6 +136,24 @@ typedef struct fmt2d_lsqr_params {
 FMT2D_API int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params, const double* residual,
                          const double* gtg_diag, const double* dm_sum, double* dm, int* iters,
                          double* rnorm, double* bnorm, double* test2);
+/* fmt2d_lsqr without any device allocation.  No counterpart in the reference
+ * (which allocates its LSQR work arrays per call).  For callers that cannot
+ * call cudaMalloc while they solve: a driver that overlaps this solve with
+ * work on other streams (cudaMalloc / cudaFree can synchronise the whole
+ * device), or a program whose device memory is reserved up front by its own
+ * pool allocator, where a new cudaMalloc fails or fragments that reserve.
+ * residual[ndata], gtg_diag[nparm] (NULL: computed), dm_sum[nparm] (NULL:
+ * zeros) and dm[nparm] are DEVICE pointers owned by the caller; G is the one
+ * set by fmt2d_set_frechet.  The work vectors live in one fixed 32 MiB device
+ * array that every GPU loading the library holds until exit; problems that
+ * need more (about ndata + 6.125 nparm doubles) are rejected with
+ * FMT2D_ERR_ARG.  The first call on a device looks up that array's address,
+ * so make it before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race. */
+FMT2D_API int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params,
+                                 const double* residual, const double* gtg_diag,
+                                 const double* dm_sum, double* dm, int* iters, double* rnorm,
+                                 double* bnorm, double* test2);
 /* Device milliseconds and kernel launches of the last fmt2d_lsqr (diagnostics,
  * no reference counterpart). */
 FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
