@@ -60,11 +60,13 @@ def lib():
     L.fmt2d_upload_model.argtypes = [V, P(ModelDesc)]
     L.fmt2d_model_info.argtypes = [V, P(C.c_int), P(C.c_int), P(C.c_double), P(C.c_double)]
     L.fmt2d_region_nodes.argtypes = [V, C.c_int, P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fmt2d_region_geometry.argtypes = [V, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_inv_index.argtypes = [V, C.c_void_p, P(C.c_int), P(C.c_int)]
     L.fmt2d_forward.argtypes = [V, _dp, C.c_int, C.c_int]
     L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
+    L.fmt2d_set_schedule.argtypes = [V, C.c_int, C.c_double, C.c_int]
     L.fmt2d_set_frechet.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int]
     L.fmt2d_spmv.argtypes = [V, C.c_int, C.c_void_p, C.c_void_p]

@@ -89,6 +89,14 @@ class Fmt2d:
                                               N.ptr(i3)), "fmt2d_region_nodes")
         return i1, i2, i3
 
+    def region_geometry(self, r: int):
+        """Node x, z and FP64 velocity of region r in the reference's order."""
+        n = self.region_nnode(r)
+        x, z, v = np.zeros(n), np.zeros(n), np.zeros(n)
+        self._check(self.L.fmt2d_region_geometry(self.h, r, N.ptr(x), N.ptr(z), N.ptr(v)),
+                    "fmt2d_region_geometry")
+        return x, z, v
+
     def region_nnode(self, r: int) -> int:
         n = C.c_int()
         self._check(self.L.fmt2d_region_nodes(self.h, r, C.byref(n), None, None, None),
@@ -172,6 +180,12 @@ class Fmt2d:
         ms, n = C.c_double(), C.c_int()
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
+
+    def set_schedule(self, inner: int = 8, window_cells: float = 4.0, steps_per_check: int = 16):
+        """Eikonal solve schedule (fmt2d_set_schedule); results do not depend on it."""
+        self._check(self.L.fmt2d_set_schedule(self.h, int(inner), float(window_cells),
+                                              int(steps_per_check)), "fmt2d_set_schedule")
+        return self
 
     def stream(self) -> int:
         """cudaStream_t (as an integer) that the context's work runs on."""

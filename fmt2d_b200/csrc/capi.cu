@@ -115,6 +115,28 @@ int fmt2d_region_nodes(fmt2d_ctx* ctx, int region, int* nnode, int* i1, int* i2,
   return FMT2D_OK;
 }
 
+int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, double* z, double* vel) {
+  if (!ctx || region < 1 || region > 6) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const fmt2d::Model& m = ctx->model;
+  const fmt2d::Region& r = m.reg[region];
+  for (int id = 0; id < r.nnode; ++id) {
+    const int s = r.slot_of_node[id];
+    if (vel) vel[id] = r.vel64[s];
+    if (id < r.ngnode) {
+      const int ix = s % r.pitch, iz = s / r.pitch + r.z_lo;
+      if (x) x[id] = m.x0 + (double)ix * m.dx;
+      if (z) z[id] = (double)iz * m.dx;
+    } else {
+      const int k = (id - r.ngnode) % m.nx;
+      const bool top = id - r.ngnode < m.nx;
+      if (x) x[id] = m.xpos[k];
+      if (z) z[id] = m.ifc[top ? r.itop : r.ibot].z[k];
+    }
+  }
+  return FMT2D_OK;
+}
+
 int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* nvp, int* npar) {
   if (!ctx) return FMT2D_ERR_ARG;
   if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
@@ -260,6 +282,18 @@ int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
   if (!ctx->need_gpu(code)) return code;
   if (ms) *ms = ctx->lsqr->last_ms();
   if (launches) *launches = ctx->lsqr->last_launches();
+  return FMT2D_OK;
+}
+
+int fmt2d_set_schedule(fmt2d_ctx* ctx, int inner, double window_cells, int steps_per_check) {
+  if (!ctx || inner < 1 || inner > 64 || !(window_cells > 0.0) || steps_per_check < 1 ||
+      steps_per_check > 256)
+    return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  ctx->eng->inner = inner;
+  ctx->eng->window_cells = window_cells;
+  ctx->eng->steps_per_check = steps_per_check;
   return FMT2D_OK;
 }
 

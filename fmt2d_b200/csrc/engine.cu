@@ -1,10 +1,10 @@
 // Host engine: model upload and the batched forward solve (all sources' time
 // fields of one stage level are solved together in one round loop).
 #include "engine.h"
-#include "kernels.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 
 namespace fmt2d {
 
@@ -86,15 +86,7 @@ Engine::Engine(int device) : device_(device) {
   cudaSetDevice(device_);
   cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
   cudaMallocHost(&h_count_, 4 * sizeof(unsigned));
-  cudaFuncSetAttribute(eik_visit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)eik_round_smem());
-  cudaFuncSetAttribute(eik_final, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)eik_round_smem());
-  // persistent visit blocks: as many warps as fit on the device at once
-  int nsm = 0, per_sm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eik_visit, 32, eik_round_smem());
-  visit_blocks_ = std::max(1, nsm) * std::max(1, per_sm);
+  step_grid_ = e64_step_grid(device_);
 }
 
 Engine::~Engine() {
@@ -122,46 +114,17 @@ std::string Engine::upload(const Model& m) {
       iz[G.pitch + k] = m.ifc[G.ibot].z[k];
     }
     if (!(e = put(D.code, G.code, stream_)).empty()) return e;
-    if (!(e = put(D.vel, G.vel, stream_)).empty()) return e;
     if (!(e = put(D.vel64, G.vel64, stream_)).empty()) return e;
-    if (!(e = put(D.iface_dz, G.iface_dz, stream_)).empty()) return e;
     if (!(e = put(D.izc, izc, stream_)).empty()) return e;
     if (!(e = put(D.iface_x, ix, stream_)).empty()) return e;
     if (!(e = put(D.iface_z, iz, stream_)).empty()) return e;
     if (!(e = put(D.r0, G.r0, stream_)).empty()) return e;
     if (!(e = put(D.r1, G.r1, stream_)).empty()) return e;
     if (!(e = put(D.slot_of_node, G.slot_of_node, stream_)).empty()) return e;
-    DevRegion& R = D.R;
-    R.code = D.code.as<uint32_t>();
-    R.vel = D.vel.as<float>();
-    R.iface_dz = D.iface_dz.as<float>();
-    R.izc = D.izc.as<int>();
-    R.H = G.H;
-    R.pitch = G.pitch;
-    R.tiles_x = G.tiles_x;
-    R.tiles_y = G.tiles_y;
-    R.z_lo = G.z_lo;
-    R.nx = m.nx;
-    R.dx = m.dx;
-    R.x0 = m.x0;
-    R.tol = m.tolerance;
-    DevRegionX& X = D.X;
-    X.vel64 = D.vel64.as<double>();
-    X.iface_x = D.iface_x.as<double>();
-    X.iface_z = D.iface_z.as<double>();
-    X.r0 = D.r0.as<int>();
-    X.r1 = D.r1.as<int>();
-    X.itop = G.itop;
-    X.ibot = G.ibot;
-    X.id = r;
-    X.nz = m.nz;
     D.nslots = G.nslots();
-    D.ntiles = G.tiles_x * G.tiles_y;
-    double vs = 0.0;
-    long nv = 0;
-    for (size_t s = 0; s < G.vel64.size(); ++s)
-      if (G.vel64[s] > 0.0) { vs += G.vel64[s]; ++nv; }
-    D.vmean = nv ? vs / nv : 1.0;
+    double vm = 0.0;
+    for (size_t s2 = 0; s2 < G.vel64.size(); ++s2) vm = std::max(vm, G.vel64[s2]);
+    D.vmax = vm > 0.0 ? vm : 1.0;
   }
   for (int k = 1; k <= 5; ++k) {
     const Interface& f = m.ifc[k];
@@ -171,7 +134,7 @@ std::string Engine::upload(const Model& m) {
     if (!(e = put(ifc_buf_[k][3], f.vel_top, stream_)).empty()) return e;
     if (!(e = put(ifc_buf_[k][4], f.vel_bot, stream_)).empty()) return e;
     if (!(e = put(ifc_buf_[k][5], f.izc, stream_)).empty()) return e;
-    DevIface& I = ifc_[k];
+    Ifc64& I = ifc_[k];
     I.z = ifc_buf_[k][0].as<double>();
     I.nrm_x = ifc_buf_[k][1].as<double>();
     I.nrm_z = ifc_buf_[k][2].as<double>();
@@ -239,17 +202,13 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
       F.solved = false;
       if (!(need & (1u << tf))) continue;
       const DevRegionStore& D = reg_[kTf[tf].reg];
-      F.t2.alloc(D.nslots * 8);
-      F.g2.alloc(D.nslots * 8);
-      F.gout.alloc(D.nslots * 8);
-      F.susp.alloc(D.nslots);
-      F.act.alloc((size_t)kTileWords * D.ntiles * 4);
-      F.tkey.alloc((size_t)D.ntiles * 8);   // keys, then visit counts
-      F.front.alloc(16);
-      F.seed.alloc(D.nslots * 16);
-      F.sflag.alloc(D.nslots);
-      if (!F.t2.p || !F.g2.p || !F.gout.p || !F.susp.p || !F.act.p || !F.seed.p || !F.sflag.p ||
-          !F.tkey.p || !F.front.p)
+      F.T.alloc(D.nslots * 8);
+      F.G.alloc(D.nslots * 16);
+      F.Gout.alloc(D.nslots * 16);
+      F.fl.alloc(D.nslots);
+      F.seed.alloc(D.nslots * 32);
+      F.clock.alloc(32);
+      if (!F.T.p || !F.G.p || !F.Gout.p || !F.fl.p || !F.seed.p || !F.clock.p)
         return "device allocation failed for the time fields";
     }
   }
@@ -267,174 +226,183 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
   return std::string();
 }
 
+Fld64 Engine::field_view(int src, int tf) const {
+  const Region& G = m_.reg[kTf[tf].reg];
+  const DevRegionStore& D = reg_[kTf[tf].reg];
+  const FieldStore& S = fields_[src][tf];
+  Fld64 f;
+  f.code = D.code.as<uint32_t>();
+  f.vel = D.vel64.as<double>();
+  f.izc = D.izc.as<int>();
+  f.ifx = D.iface_x.as<double>();
+  f.ifz = D.iface_z.as<double>();
+  f.H = G.H;
+  f.pitch = G.pitch;
+  f.z_lo = G.z_lo;
+  f.nx = m_.nx;
+  f.nz = m_.nz;
+  f.x0 = m_.x0;
+  f.dx = m_.dx;
+  f.tol = m_.tolerance;
+  f.T = S.T.as<double>();
+  f.G = S.G.as<double2>();
+  f.Gout = S.Gout.as<double2>();
+  f.fl = S.fl.as<uint8_t>();
+  f.seed = S.seed.as<double4>();
+  f.clock = S.clock.as<double>();
+  return f;
+}
+
 std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   const int nf = (int)items.size();
-  std::vector<DevField> hf(nf);
-  std::vector<DevRegionX> hx(nf);
-  std::vector<float*> hg(nf);
-  std::vector<uint8_t*> hs(nf);
-  std::vector<int> up(nf, -1);
-  std::vector<int> hw;
-  int total_tiles = 0;
-  size_t max_slots = 0;
+  std::vector<Fld64> hf(nf);
+  std::vector<int> up(nf, -1), hw;
+  std::vector<double> wstep(nf);
+  size_t total = 0, max_slots = 0;
   for (int i = 0; i < nf; ++i) {
     const int s = items[i].first, tf = items[i].second;
     const DevRegionStore& D = reg_[kTf[tf].reg];
-    FieldStore& F = fields_[s][tf];
-    DevField& f = hf[i];
-    f.R = D.R;
-    f.Th = F.t2.as<float>();
-    f.Tl = f.Th;
-    f.gx = F.g2.as<float>();
-    f.gz = f.gx;
-    f.act = F.act.as<unsigned>();
-    f.tkey = F.tkey.as<unsigned>();
-    f.tvis = f.tkey + reg_[kTf[tf].reg].ntiles;
-    f.front = F.front.as<float>();
-    f.band = (float)(band_tiles * kTW * m_.dx / D.vmean);
-    f.seed = F.seed.as<float4>();
-    f.sflag = F.sflag.as<uint8_t>();
-    f.frozen_slot = -1;
-    f.tile_base = total_tiles;
-    total_tiles += D.ntiles;
+    hf[i] = field_view(s, tf);
+    hf[i].gbase = (unsigned)total;
+    total += D.nslots;
     max_slots = std::max(max_slots, D.nslots);
-    hx[i] = D.X;
-    hg[i] = F.gout.as<float>();
-    hs[i] = F.susp.as<uint8_t>();
     up[i] = kTf[tf].water_up;
+    wstep[i] = window_cells * m_.dx / D.vmax;
     if (tf == 5) hw.push_back(i);
   }
+  if (total >= 0xffffffffull) return "batch too large for 32-bit node ids";
   std::string e;
   if (!(e = put(d_fields_, hf, stream_)).empty()) return e;
-  if (!(e = put(d_xs_, hx, stream_)).empty()) return e;
-  if (!(e = put(d_gout_, hg, stream_)).empty()) return e;
-  if (!(e = put(d_susp_, hs, stream_)).empty()) return e;
   if (!(e = put(d_up_, up, stream_)).empty()) return e;
-  DevField* dF = d_fields_.as<DevField>();
-  {
-    const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 1024);
-    k_fill<<<dim3(bx, nf), 256, 0, stream_>>>(dF, nf, max_slots);
-    ++stats_.launches;
-    CK(cudaGetLastError());
-  }
+  if (!(e = put(d_step_, wstep, stream_)).empty()) return e;
+  // three lists (read, written, emptied) rotate through the steps
+  d_list_.alloc(3 * total * sizeof(unsigned));
+  d_inq_.alloc(((total + 31) / 32) * sizeof(unsigned));
+  d_count_.alloc(8 * sizeof(unsigned));
+  d_done_.alloc(16);
+  d_ctr_.alloc(4 * sizeof(unsigned long long));
+  if (!d_list_.p || !d_inq_.p || !d_count_.p || !d_done_.p || !d_ctr_.p)
+    return "device allocation failed for the active lists";
+  unsigned* L[3] = {d_list_.as<unsigned>(), d_list_.as<unsigned>() + total,
+                    d_list_.as<unsigned>() + 2 * total};
+  unsigned* cnt = d_count_.as<unsigned>();    // [0..2] list lengths, [3] check result
+  unsigned long long* dctr = d_ctr_.as<unsigned long long>();
+  CK(cudaMemsetAsync(d_inq_.p, 0, ((total + 31) / 32) * sizeof(unsigned), stream_));
+  CK(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned), stream_));
+  CK(cudaMemsetAsync(d_done_.p, 0, 16, stream_));
+  CK(cudaMemsetAsync(dctr, 0, 4 * sizeof(unsigned long long), stream_));
+  Fld64* dF = d_fields_.as<Fld64>();
+  e64_fill(dF, nf, max_slots, stream_);
+  ++stats_.launches;
+  CK(cudaGetLastError());
   const int level = kTf[items[0].second].level;
   if (level == 0) {
     std::vector<double> sx(nf), sz(nf);
     for (int i = 0; i < nf; ++i) { sx[i] = src_x_[items[i].first]; sz[i] = src_z_[items[i].first]; }
     if (!(e = put(d_sx_, sx, stream_)).empty()) return e;
     if (!(e = put(d_sz_, sz, stream_)).empty()) return e;
-    k_init_source<<<(nf + 63) / 64, 64, 0, stream_>>>(dF, d_xs_.as<DevRegionX>(),
-                                                       d_sx_.as<double>(), d_sz_.as<double>(),
-                                                       nf, m_.nz);
+    e64_init_source(dF, d_sx_.as<double>(), d_sz_.as<double>(), nf, stream_);
     ++stats_.launches;
-    CK(cudaGetLastError());
   } else {
-    std::vector<SeedDesc> sd(nf);
+    std::vector<Seed64> sd(nf);
     for (int i = 0; i < nf; ++i) {
       const int s = items[i].first, tf = items[i].second;
       const TfInfo& I = kTf[tf];
       const FieldStore& P = fields_[s][I.parent];
       if (!P.solved) return "parent time field not solved";
       const Region& PR = m_.reg[kTf[I.parent].reg];
-      SeedDesc& d = sd[i];
-      d.dst = hf[i];
-      d.dstx = hx[i];
-      d.src_t = P.t2.as<float>();
-      d.src_g = P.gout.as<float>();
+      const DevRegionStore& D = reg_[I.reg];
+      Seed64& d = sd[i];
+      d.dst = i;
+      d.src_T = P.T.as<double>();
+      d.src_G = P.Gout.as<double2>();
       d.src_row = PR.H + (I.istart == PR.itop ? 0 : 1);
       d.src_pitch = PR.pitch;
       d.ifc = ifc_[I.istart];
+      d.r0 = D.r0.as<int>();
+      d.r1 = D.r1.as<int>();
       d.dst_side = I.dst_side;
       d.reflect = I.reflect;
       d.target_side = I.target_side;
     }
     if (!(e = put(d_seeds_, sd, stream_)).empty()) return e;
-    k_seed_iface<<<dim3((m_.nx + 127) / 128, nf), 128, 0, stream_>>>(d_seeds_.as<SeedDesc>(), nf,
-                                                                    m_.nz);
+    e64_seed_iface(dF, d_seeds_.as<Seed64>(), nf, m_.nx, stream_);
     ++stats_.launches;
-    CK(cudaGetLastError());
   }
-  d_count_.alloc(16);
-  d_counters_.alloc(4 * sizeof(unsigned long long));
-  unsigned long long* dctr = d_counters_.as<unsigned long long>();
-  CK(cudaMemsetAsync(dctr, 0, 4 * sizeof(unsigned long long), stream_));
-  unsigned* dcount = d_count_.as<unsigned>();
-  const size_t smem = eik_round_smem();
-  d_queue_.alloc((size_t)total_tiles * sizeof(unsigned));
-  unsigned* dq = d_queue_.as<unsigned>();
-  {
-    const int bx = (int)std::min<size_t>(((size_t)kTileWords * 4096 + 255) / 256, 256);
-    k_seed_masks<<<dim3(bx, nf), 256, 0, stream_>>>(dF, nf);
-    ++stats_.launches;
-    CK(cudaGetLastError());
+  e64_start(dF, nf, max_slots, d_step_.as<double>(), L[0], cnt + 0, d_inq_.as<unsigned>(),
+            stream_);
+  stats_.launches += 2;
+  CK(cudaGetLastError());
+  // the step loop: graphs of steps_per_check steps (a multiple of 3, so every
+  // graph starts reading list 0), then the length of list 0 comes back
+  const int spc = std::max(3, steps_per_check / 3 * 3);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < spc; ++k) {
+    const int a = k % 3, b = (k + 1) % 3, c = (k + 2) % 3;
+    e64_step(dF, nf, L[a], cnt + a, L[b], cnt + b, cnt + c, d_inq_.as<unsigned>(),
+             d_done_.as<unsigned>(), step_grid_, dctr, stream_);
   }
+  CK(cudaMemcpyAsync(h_count_, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamEndCapture(stream_, &graph));
+  CK(cudaGraphInstantiate(&exec, graph, 0));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int pass = 0; pass < 6; ++pass) {
-    for (int round = 0; round < max_rounds; ++round) {
-      // dcount: [0] tiles with pending work, [1] queued tiles, [2] queue head
-      CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
-      eik_front<<<nf, 256, 0, stream_>>>(dF, nf, dcount);
-      ++stats_.launches;
-      eik_select<<<(total_tiles + 255) / 256, 256, 0, stream_>>>(dF, nf, total_tiles, dq,
-                                                                 dcount + 1);
-      ++stats_.launches;
-      cudaEventRecord(e0, stream_);
-      eik_visit<<<visit_blocks_, 32, smem, stream_>>>(dF, nf, dq, dcount + 1, dcount + 2,
-                                                      max_passes, dctr);
-      ++stats_.launches;
-      cudaEventRecord(e1, stream_);
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(h_count_, dcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
-                         stream_));
-      CK(cudaStreamSynchronize(stream_));
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      stats_.round_ms += ms;
-      ++stats_.rounds;
-      stats_.tile_visits += h_count_[1];
-      if (h_count_[0] == 0u) break;
-    }
-    CK(cudaMemsetAsync(dcount, 0, 4 * sizeof(unsigned), stream_));
-    eik_final<<<total_tiles, 32, smem, stream_>>>(dF, nf, d_gout_.as<float*>(),
-                                                  d_susp_.as<uint8_t*>(), dcount);
-    ++stats_.launches;
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h_count_, dcount, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
+  cudaEventRecord(e0, stream_);
+  long long steps = 0;
+  int verify_passes = 0;
+  std::string err;
+  for (;;) {
+    const cudaError_t ge = cudaGraphLaunch(exec, stream_);
+    if (ge != cudaSuccess) { err = std::string("cudaGraphLaunch: ") + cudaGetErrorString(ge); break; }
+    steps += spc;
+    stats_.launches += spc;
+    const cudaError_t se = cudaStreamSynchronize(stream_);
+    if (se != cudaSuccess) { err = std::string("step loop: ") + cudaGetErrorString(se); break; }
+    if (steps >= max_steps) { err = "eikonal solve did not converge within the step cap"; break; }
+    if (h_count_[0] != 0u) continue;
+    // empty list: check the fixed point of every node, resume if needed
+    if (verify_passes >= 6) break;   // nodes still moving are reported in the stats
+    ++verify_passes;
     ++stats_.final_passes;
+    cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned), stream_);
+    e64_verify(dF, nf, max_slots, L[0], cnt + 0, d_inq_.as<unsigned>(), cnt + 3, stream_);
+    ++stats_.launches;
+    cudaMemcpyAsync(h_count_, cnt + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_);
+    const cudaError_t ve = cudaStreamSynchronize(stream_);
+    if (ve != cudaSuccess) { err = std::string("fixed-point check: ") + cudaGetErrorString(ve); break; }
+    stats_.capped = h_count_[0];
     if (h_count_[0] == 0u) break;
   }
+  cudaEventRecord(e1, stream_);
+  cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (!err.empty()) return err;
+  stats_.round_ms += ms;
+  stats_.rounds += (int)steps;
   {
     unsigned long long c[4];
     CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
-    stats_.passes += c[0];
-    stats_.steps += c[1];
-    stats_.capped += c[2];
-    stats_.updates += c[3];
+    stats_.updates += c[0];
+    stats_.passes += c[1];
+    stats_.steps += steps / spc;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  {
-    const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 512);
-    k_fit_suspect<<<dim3(bx, nf), 256, 0, stream_>>>(dF, d_xs_.as<DevRegionX>(),
-                                                     d_gout_.as<float*>(), d_susp_.as<uint8_t*>(),
-                                                     nf);
-    ++stats_.launches;
-    CK(cudaGetLastError());
-    k_water_fix<<<dim3((m_.nx + 127) / 128, nf), 128, 0, stream_>>>(dF, d_gout_.as<float*>(),
-                                                                   d_up_.as<int>(), nf);
-    ++stats_.launches;
-    CK(cudaGetLastError());
-  }
+  e64_finish(dF, nf, max_slots, d_up_.as<int>(), stream_);
+  stats_.launches += 2;
+  CK(cudaGetLastError());
   if (!hw.empty()) {
     if (!(e = put(d_which_, hw, stream_)).empty()) return e;
     d_scratch_.alloc(hw.size() * (size_t)m_.nx * sizeof(double));
     const double dx_if = m_.xpos[1] - m_.xpos[0];
-    k_headwave<<<((int)hw.size() + 31) / 32, 32, 0, stream_>>>(
-        dF, d_xs_.as<DevRegionX>(), d_gout_.as<float*>(), hw_slot_.as<int>(), hw_v_.as<double>(),
-        dx_if, m_.nx, d_scratch_.as<double>(), d_which_.as<int>(), (int)hw.size());
+    e64_headwave(dF, hw_slot_.as<int>(), hw_v_.as<double>(), dx_if, m_.nx,
+                 d_scratch_.as<double>(), d_which_.as<int>(), (int)hw.size(), stream_);
     ++stats_.launches;
     CK(cudaGetLastError());
   }
@@ -459,9 +427,8 @@ std::string Engine::get_field(int src, int tf, double* T, double* gx, double* gz
   out.alloc((size_t)nn * 3 * sizeof(double));
   if (!out.p) return "device allocation failed";
   double* d = out.as<double>();
-  k_export<<<(nn + 255) / 256, 256, 0, stream_>>>(F.t2.as<float>(), F.gout.as<float>(),
-                                                  D.slot_of_node.as<int>(), nn, d, d + nn,
-                                                  d + 2 * (size_t)nn);
+  e64_export(F.T.as<double>(), F.Gout.as<double2>(), D.slot_of_node.as<int>(), nn, d, d + nn,
+             d + 2 * (size_t)nn, stream_);
   ++stats_.launches;
   CK(cudaGetLastError());
   if (T) CK(cudaMemcpyAsync(T, d, nn * sizeof(double), cudaMemcpyDeviceToHost, stream_));

@@ -6,7 +6,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "fields.cuh"
+#include "eik64.cuh"
 #include "model.h"
 
 namespace fmt2d {
@@ -29,26 +29,25 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Static device data of one region (slot layout of model.h).
 struct DevRegionStore {
-  DevBuf code, vel, vel64, iface_dz, izc, iface_x, iface_z, r0, r1, slot_of_node;
-  DevRegion R;
-  DevRegionX X;
+  DevBuf code, vel64, izc, iface_x, iface_z, r0, r1, slot_of_node;
   size_t nslots = 0;
-  int ntiles = 0;
-  double vmean = 1.0;   // mean region velocity (sets the processing band)
+  double vmax = 1.0;   // largest region velocity (sets the window step)
 };
 
+// One solved (source, time field): FP64 time and final gradient per slot,
+// plus the solver state of the field.
 struct FieldStore {
-  DevBuf t2, g2, gout, susp, act, seed, sflag, tkey, front;
+  DevBuf T, G, Gout, fl, seed, clock;
   bool solved = false;
 };
 
 struct SolveStats {
   int rounds = 0, batches = 0, final_passes = 0;
   long long tile_visits = 0;
-  double round_ms = 0.0;     // device time of the round kernels
-  // device counters: sweep passes, warp row/column steps, visits that hit
-  // the pass cap, node updates
+  double round_ms = 0.0;     // device time of the step kernels
+  // node evaluations, writes, graph launches
   unsigned long long passes = 0, steps = 0, capped = 0, updates = 0;
   long long launches = 0;     // kernels launched since the last forward began
   long long nodes = 0;        // region nodes of the time fields solved
@@ -66,12 +65,13 @@ class Engine {
   const Model& model() const { return m_; }
   cudaStream_t stream() const { return stream_; }
   const SolveStats& stats() const { return stats_; }
-  int max_passes = 64;     // directional sweeps per tile visit before it re-queues itself
-  double band_tiles = 1.5; // processing band: this many tile widths at the mean velocity
-  int max_rounds = 4000;   // safety cap on rounds per batch
-  // device pointers of a solved field (float2 time, float2 gradient per slot)
-  const float* field_t(int src, int tf) const { return fields_[src][tf].t2.as<float>(); }
-  const float* field_g(int src, int tf) const { return fields_[src][tf].gout.as<float>(); }
+  int inner = 1;             // unused by the list schedule (kept for the C ABI)
+  double window_cells = 4.0; // window step: this many cells at the region's largest velocity
+  int steps_per_check = 24;  // steps per captured graph between list checks (multiple of 3)
+  long long max_steps = 200000;   // safety cap on steps per level
+  // device pointers of a solved field (FP64 time, double2 final gradient per slot)
+  const double* field_t(int src, int tf) const { return fields_[src][tf].T.as<double>(); }
+  const double2* field_g(int src, int tf) const { return fields_[src][tf].Gout.as<double2>(); }
   const DevRegionStore& region(int r) const { return reg_[r]; }
   double source_z(int src) const { return src_z_[src]; }
   double source_x(int src) const { return src_x_[src]; }
@@ -80,19 +80,20 @@ class Engine {
  private:
   std::string solve_level(const std::vector<std::pair<int, int>>& items);
   void ensure_sources(int nsrc);
+  Fld64 field_view(int src, int tf) const;
   int device_;
   cudaStream_t stream_ = nullptr;
   Model m_;
   DevRegionStore reg_[7];
   DevBuf ifc_buf_[6][6];      // z, nx, nz, vel_top, vel_bot, izc
-  DevIface ifc_[6];
+  Ifc64 ifc_[6];
   DevBuf hw_slot_, hw_v_;
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
-  DevBuf d_fields_, d_xs_, d_seeds_, d_sx_, d_sz_, d_count_, d_gout_, d_susp_, d_up_, d_which_,
-      d_scratch_, d_counters_, d_queue_;
+  DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_count_, d_scratch_, d_which_, d_up_, d_step_,
+      d_done_, d_ctr_, d_list_, d_inq_;
   unsigned* h_count_ = nullptr;
-  int visit_blocks_ = 1;
+  int step_grid_ = 1;
   SolveStats stats_;
 };
 

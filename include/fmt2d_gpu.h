@@ -87,6 +87,10 @@ FMT2D_API int fmt2d_model_info(fmt2d_ctx* ctx, int* nx, int* nz, double* dx, dou
  * table (i1 = grid column 1-based or 0 for interface nodes, i2 = grid row
  * 1-based or interface id, i3 = interface node index 1-based or 0). */
 FMT2D_API int fmt2d_region_nodes(fmt2d_ctx* ctx, int region, int* nnode, int* i1, int* i2, int* i3);
+/* Region r (1..6): node positions and P velocity in the reference's node order
+ * (Tregion2d%x, %z, %velocity of propagate2d.f90:1564-1647, FP64); any array
+ * may be NULL.  These are the exact doubles the device stencil computes with. */
+FMT2D_API int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, double* z, double* vel);
 /* Inversion parameter numbering (frechet2d.f90:55-63): inv_idx[nx*nz] with ix
  * fastest, 1-based ids, 0 inactive; returns counts. */
 FMT2D_API int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* n_vel_parms, int* n_inv_parms);
@@ -157,6 +161,13 @@ FMT2D_API int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params
 /* Device milliseconds and kernel launches of the last fmt2d_lsqr (diagnostics,
  * no reference counterpart). */
 FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
+
+/* Schedule of the eikonal solve (no reference counterpart; the reference's
+ * heap has no schedule): relaxation rounds per tile visit (1..64), the time
+ * window's step in cells at the region's largest velocity (> 0), and steps
+ * between convergence checks (1..256).  Results do not depend on them. */
+FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, int inner, double window_cells,
+                                 int steps_per_check);
 
 /* The CUDA stream (cudaStream_t) all work of the context is issued on, for
  * callers that record events around fmt2d_forward.  No reference counterpart. */

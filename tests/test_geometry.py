@@ -30,6 +30,12 @@ def test_region_and_parameter_numbering(oracle_lib, native, which):
         np.testing.assert_array_equal(i1, R["i1"])
         np.testing.assert_array_equal(i2, R["i2"])
         np.testing.assert_array_equal(i3, R["i3"])
+        # positions and velocities are the doubles the FP64 stencil uses:
+        # they must be bit-identical to the restatement's
+        x, z, v = g.region_geometry(r)
+        np.testing.assert_array_equal(x, R["x"])
+        np.testing.assert_array_equal(z, R["z"])
+        np.testing.assert_array_equal(v, R["vel"])
     inv_o, nvp_o, np_o = o.inv_idx()
     inv_g, nvp_g, np_g = g.inv_index()
     np.testing.assert_array_equal(inv_g, inv_o)
