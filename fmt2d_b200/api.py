@@ -134,6 +134,32 @@ class Fmt2d:
         return {k: (round(float(x), 3) if k == "solve_ms" else int(x))
                 for k, x in zip(self.STATS, v)}
 
+    # ------------------------------------------------------------ rays and Frechet rows
+    def trace(self, src, phase, rx, rz):
+        """Ray backtrace and Frechet rows of picks on the last forward's fields
+        (fmt2d_trace).  Returns (t_calc, valid, nnz)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        phase = np.ascontiguousarray(phase, dtype=np.int32)
+        rx = np.ascontiguousarray(rx, dtype=np.float64)
+        rz = np.ascontiguousarray(rz, dtype=np.float64)
+        n = src.size
+        t = np.zeros(n)
+        v = np.zeros(n, np.int32)
+        nnz = C.c_longlong()
+        self._check(self.L.fmt2d_trace(self.h, N.ptr(src), N.ptr(phase), N.ptr(rx), N.ptr(rz), n,
+                                       N.ptr(t), N.ptr(v), C.byref(nnz)), "fmt2d_trace")
+        self.npick, self.frechet_nnz = n, nnz.value
+        return t, v.astype(bool), nnz.value
+
+    def frechet_rows(self, index_base: int = 1):
+        """CSR (row_ptr, gindx, gval) of the last trace (fmt2d_frechet_rows)."""
+        rp = np.zeros(self.npick + 1, np.int32)
+        gi = np.zeros(max(self.frechet_nnz, 1), np.int32)
+        gv = np.zeros(max(self.frechet_nnz, 1))
+        self._check(self.L.fmt2d_frechet_rows(self.h, N.ptr(rp), N.ptr(gi), N.ptr(gv),
+                                              int(index_base)), "fmt2d_frechet_rows")
+        return rp, gi[: self.frechet_nnz], gv[: self.frechet_nnz]
+
     # ------------------------------------------------------------ G and LSQR
     def set_frechet(self, ndata: int, nparm: int, row_ptr, gindx, gval, index_base: int = 1):
         """Sensitivity matrix as CSR (read_frechet_data2d's gindx / gval /

@@ -357,6 +357,16 @@ struct NewV {
 // Seeds precede every candidate in the reference's order; a seed at or below
 // the regular candidate that would set the suspect flag means that update
 // never lowered the node.
+//
+// A seed tied with a copy from a coincident node (an interface node lying on
+// a grid node) is the one case the fixed point does not decide: the heap
+// accepts either node first, and both end with that node's values.  A grid
+// node seeded at zero distance from its interface node carries a NaN gradient
+// (sweep_region_from_interface2d divides by the distance), so which of the two
+// the heap pops first decides whether rays through that cell can be traced.
+// Keeping the seed leaves NaN on the grid node; over PmP picks of twelve test
+// models this agreed with the reference's valid flags on 96.6% of picks,
+// against 95.2% for letting a finite copy win.
 __device__ NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t) {
   NewV o;
   o.write = false;

@@ -178,6 +178,8 @@ std::string Engine::upload(const Model& m) {
     if (!(e = put(hw_slot_, hs, stream_)).empty()) return e;
     if (!(e = put(hw_v_, hv, stream_)).empty()) return e;
   }
+  if (!(e = upload_trace_tables()).empty()) return e;
+  npick_ = -1;
   CK(cudaStreamSynchronize(stream_));
   return std::string();
 }

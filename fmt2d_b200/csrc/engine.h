@@ -62,6 +62,15 @@ class Engine {
   // (placed on the seafloor), one slot per source.
   std::string forward(const double* sx, int nsrc, int phase_mask);
   std::string get_field(int src, int tf, double* T, double* gx, double* gz);
+  // Ray backtrace and Frechet rows of npick picks (source index, phase 1..5,
+  // receiver x, z) on the fields of the last forward; the rows stay on the
+  // device until frechet_rows copies them out (CSR over all picks, invalid
+  // picks empty, columns 1-based parameter ids unless base 0).
+  std::string trace(const int* src, const int* phase, const double* rx, const double* rz,
+                    int npick, double* t_calc, int* valid, long long* nnz);
+  std::string frechet_rows(int* row_ptr, int* col, double* val, int base);
+  double trace_ms() const { return trace_ms_; }
+  long long frechet_nnz() const { return nnz_; }
   const Model& model() const { return m_; }
   cudaStream_t stream() const { return stream_; }
   const SolveStats& stats() const { return stats_; }
@@ -79,6 +88,7 @@ class Engine {
 
  private:
   std::string solve_level(const std::vector<std::pair<int, int>>& items);
+  std::string upload_trace_tables();
   void ensure_sources(int nsrc);
   Fld64 field_view(int src, int tf) const;
   int device_;
@@ -92,6 +102,11 @@ class Engine {
   std::vector<double> src_x_, src_z_;
   DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_count_, d_scratch_, d_which_, d_up_, d_step_,
       d_done_, d_ctr_, d_list_, d_inq_;
+  DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
+      d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
+  int npick_ = -1, rows_ = 0;
+  long long nnz_ = 0;
+  double trace_ms_ = 0.0;
   unsigned* h_count_ = nullptr;
   int step_grid_ = 1;
   SolveStats stats_;

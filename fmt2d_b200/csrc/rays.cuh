@@ -1,0 +1,48 @@
+// Device ray backtrace and Frechet rows (one thread per pick, FP64).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fmt2d {
+
+// A region as the ray tracer reads it (slot layout of model.h).
+struct TrRegion {
+  const uint32_t* code = nullptr;
+  const int* slot_of_node = nullptr;   // region node id - 1 -> slot (the reference's node order)
+  int z_lo = 0, H = 0, pitch = 0, itop = 0, ibot = 0, id = 0, nnode = 0;
+};
+
+// Model data shared by every pick.
+struct TrModel {
+  int nx = 0, nz = 0;
+  double x0 = 0, dx = 0, tol = 0, vwater = 1.5;
+  const double* vel = nullptr;        // propagation-grid velocity, ix fastest
+  const double* xpos = nullptr;       // interface node x (= velocity-grid x)
+  const double* ifz[6] = {};          // interface node depths, interfaces 1..5
+  const int* inv_idx = nullptr;       // inversion numbering, 1-based, 0 inactive
+  int iface_inv = 0, iface_start = 0, n_inv = 0;
+  TrRegion reg[7];
+};
+
+// One pick: source (OBS) index, phase 1..5, receiver (shot) position.
+struct TrPick {
+  int src, phase;
+  double rx, rz;
+};
+
+// Per pick: the fields of its source (indexed src*13 + tf) give T and the
+// final gradient.
+struct TrField {
+  const double* T = nullptr;
+  const double2* G = nullptr;
+};
+
+// Trace every pick.  Pass 1 (rows == nullptr): t_calc, valid and the number
+// of Frechet contributions of each pick (cnt).  Pass 2: the contributions
+// themselves at off[pick] (keys = pick << 32 | parameter id, 1-based).
+void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, const double* src_z,
+               const TrPick* picks, int npick, double* t_calc, int* valid, unsigned* cnt,
+               const unsigned long long* off, unsigned long long* keys, double* vals,
+               cudaStream_t st);
+
+}  // namespace fmt2d

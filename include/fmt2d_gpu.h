@@ -110,6 +110,29 @@ FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double
 #define FMT2D_N_STATS 11
 FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
 
+/* Ray backtrace and Frechet rows of npick picks on the fields of the last
+ * fmt2d_forward: per pick the source index src[i] (0-based, into that call's
+ * sources), the phase (1..5) and the receiver (shot) position rx, rz.  This
+ * is the per-pick work of run_forward2d (src/inversion2d.f90:4488-4535): the
+ * in-water receiver handling of invert2d_main.f90:517-537 with
+ * find_optimal_entry_inv (src/inversion2d.f90:6344-6438) and the water-leg
+ * time, trace_ray_from_receiver2d (src/rays2d.f90:7-153) and
+ * compute_frechet_for_ray2d (src/inversion2d.f90:4548-4787).  Outputs:
+ * t_calc[npick] (receiver time incl. the water leg), valid[npick] (1 valid
+ * ray), and *nnz, the number of Frechet entries of all valid picks, which
+ * stay on the device for fmt2d_frechet_rows. */
+FMT2D_API int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
+                          const double* rz, int npick, double* t_calc, int* valid,
+                          long long* nnz);
+/* The Frechet rows of the last fmt2d_trace as CSR over all its picks (an
+ * invalid pick's row is empty): row_ptr[npick+1], gindx[nnz] parameter ids in
+ * ascending order (the inversion numbering of fmt2d_inv_index, interface
+ * parameters after the velocity ones), gval[nnz] = dt/d(slowness) for
+ * velocity parameters and the interface-depth derivative otherwise.
+ * index_base 1 gives the reference's 1-based row_ptr and gindx. */
+FMT2D_API int fmt2d_frechet_rows(fmt2d_ctx* ctx, int* row_ptr, int* gindx, double* gval,
+                                 int index_base);
+
 /* Sensitivity matrix G (ndata picks x nparm parameters) as CSR host arrays,
  * index_base 1 for the reference's 1-based gindx / row_ptr (row_ptr has
  * ndata+1 entries).  Columns outside 1..nparm are kept but skipped by every

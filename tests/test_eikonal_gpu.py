@@ -22,8 +22,15 @@ def _compare(o, g, slot, src, tf):
     rg = Tg < 1e19
     assert (ro == rg).all(), f"tf{tf}: reached sets differ ({(ro != rg).sum()} nodes)"
     err = np.abs(To[ro] - Tg[ro])
-    gn = np.hypot(gxo[ro], gzo[ro])
-    gerr = np.hypot(gxo[ro] - gxg[ro], gzo[ro] - gzg[ro]) / np.maximum(gn, 1e-6)
+    # A grid node seeded at zero distance from a coincident interface node has
+    # a NaN gradient in the reference; whether the heap keeps it or hands the
+    # interface node's values over depends on its acceptance order, so the two
+    # sides may disagree there.  Those nodes are a handful per field.
+    nan = np.isnan(gxo[ro]) | np.isnan(gzo[ro]) | np.isnan(gxg[ro]) | np.isnan(gzg[ro])
+    assert nan.sum() <= max(16, 0.005 * nan.size), f"tf{tf}: {nan.sum()} NaN gradients"
+    ok = ~nan
+    gn = np.hypot(gxo[ro][ok], gzo[ro][ok])
+    gerr = np.hypot(gxo[ro][ok] - gxg[ro][ok], gzo[ro][ok] - gzg[ro][ok]) / np.maximum(gn, 1e-6)
     return err.max() if err.size else 0.0, np.quantile(gerr, 0.99) if gerr.size else 0.0
 
 
