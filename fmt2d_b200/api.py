@@ -124,8 +124,8 @@ class Fmt2d:
                     "fmt2d_get_field")
         return T, gx, gz
 
-    STATS = ("rounds", "batches", "final_passes", "tile_visits", "solve_ms", "launches",
-             "nodes", "passes", "steps", "capped", "updates")
+    STATS = ("steps", "batches", "checks", "passed", "solve_ms", "launches", "nodes",
+             "evals", "graphs", "capped", "writes", "unsettled")
 
     def stats(self) -> dict:
         """Counters of the last forward (fmt2d_stats)."""
@@ -207,8 +207,10 @@ class Fmt2d:
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
 
-    def set_schedule(self, inner: int = 8, window_cells: float = 4.0, steps_per_check: int = 16):
-        """Eikonal solve schedule (fmt2d_set_schedule); results do not depend on it."""
+    def set_schedule(self, inner: int = 1, window_cells: float = 0.5, steps_per_check: int = 24):
+        """Eikonal solve schedule (fmt2d_set_schedule).  The time window bounds
+        how far ahead of the settled times a node may be written; the default
+        (0.5 cells) is the one the parity tests use."""
         self._check(self.L.fmt2d_set_schedule(self.h, int(inner), float(window_cells),
                                               int(steps_per_check)), "fmt2d_set_schedule")
         return self

@@ -172,10 +172,10 @@ int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
   const fmt2d::SolveStats& s = ctx->eng->stats();
-  const double v[FMT2D_N_STATS] = {(double)s.rounds,   (double)s.batches, (double)s.final_passes,
-                                   (double)s.tile_visits, s.round_ms,     (double)s.launches,
-                                   (double)s.nodes,    (double)s.passes,  (double)s.steps,
-                                   (double)s.capped,   (double)s.updates};
+  const double v[FMT2D_N_STATS] = {
+      (double)s.rounds,  (double)s.batches, (double)s.final_passes, (double)s.passed,
+      s.round_ms,        (double)s.launches, (double)s.nodes,       (double)s.evals,
+      (double)s.graphs,  (double)s.capped,  (double)s.writes,       (double)s.unsettled};
   for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
   return FMT2D_OK;
 }

@@ -503,7 +503,16 @@ struct Queue {
   unsigned* out_cnt;
   unsigned* sbuf;                // shared: this warp's staged appends
   unsigned* scnt;                // shared: their count
+  unsigned* ver = nullptr;       // input version per node (bumped when a node it reads changes)
 };
+
+// Input version of a node, read before its inputs (acquire: a writer bumps it
+// after a fence that follows its write).
+__device__ __forceinline__ unsigned ld_ver(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ void push_id(const Queue& q, unsigned gid) {
   const unsigned bit = 1u << (gid & 31);
@@ -532,12 +541,16 @@ __device__ __forceinline__ void flush(const Queue& q) {
 // Every candidate of a node u that involves node n (as a member, a neighbour
 // or a second-order neighbour) is at or above n's time, so a change of n
 // from time a to b can only move nodes whose time is at or above min(a, b).
-// thr is that bound; nodes below it are not re-queued.
+// thr is that bound; nodes stored below it are not re-queued.  Their input
+// version moves all the same: a deferred node's stored time is not the one
+// it waits with, so its record must not outlive the change.
 __device__ __forceinline__ void queue_grid(const Fld64& F, const Queue& q, int r, int c,
                                            double thr) {
   if (r < 0 || r >= F.H || c < 0 || c >= F.nx) return;
   const int s = r * F.pitch + c;
-  if (!(__ldg(F.code + s) & kInRegion) || ldT(F, s) < thr) return;
+  if (!(__ldg(F.code + s) & kInRegion)) return;
+  if (q.ver) atomicAdd(q.ver + F.gbase + s, 1u);
+  if (ldT(F, s) < thr) return;
   push_id(q, F.gbase + (unsigned)s);
 }
 
@@ -545,6 +558,7 @@ __device__ __forceinline__ void queue_iface(const Fld64& F, const Queue& q, int 
                                             double thr) {
   if (c < 0 || c >= F.nx) return;
   const int s = (F.H + side) * F.pitch + c;
+  if (q.ver) atomicAdd(q.ver + F.gbase + s, 1u);
   if (ldT(F, s) < thr) return;
   push_id(q, F.gbase + (unsigned)s);
 }
@@ -610,13 +624,21 @@ __device__ __forceinline__ void spread(const Fld64& F, const Queue& q, int slot,
 
 // One step: every listed node is evaluated once (a thread per node).  A new
 // time inside the field's window is written and the nodes it can move are
-// queued; one beyond the window is deferred (the node re-queues itself).  The
-// last block to finish moves on the window of every field in which nothing
-// changed during the step.  ctr: [0] evaluations, [1] writes.
+// queued; one beyond the window is deferred (the node re-queues itself and
+// records the time with the input version it was computed from, so that
+// until the window reaches that time or an input changes, listing it costs
+// a compare instead of an evaluation).  The last block to finish moves on
+// the window of every field in which nothing changed during the step.  A
+// window may take many steps to settle (a front nearly parallel to a grid
+// line puts a whole line of nodes, each waiting for the next, into one
+// window); moving it earlier would accept times that are not final.
+// ctr: [0] evaluations, [1] writes, [2] deferred nodes passed over.
+
 __global__ void __launch_bounds__(32 * kQWarps) k_step(Fld64* fields, int nf, const unsigned* in,
                                                        const unsigned* in_cnt, unsigned* out,
                                                        unsigned* out_cnt, unsigned* zero_cnt,
                                                        unsigned* inq, unsigned* done,
+                                                       unsigned* ver, unsigned long long* pend,
                                                        unsigned long long* ctr) {
   __shared__ unsigned s_buf[kQWarps][kQBuf];
   __shared__ unsigned s_cnt[kQWarps];
@@ -630,9 +652,10 @@ __global__ void __launch_bounds__(32 * kQWarps) k_step(Fld64* fields, int nf, co
   q.out_cnt = out_cnt;
   q.sbuf = s_buf[wib];
   q.scnt = s_cnt + wib;
+  q.ver = ver;
   const unsigned n = __ldcg(in_cnt);
   const unsigned warp = blockIdx.x * kQWarps + wib, nwarp = gridDim.x * kQWarps;
-  unsigned long long n_eval = 0, n_write = 0;
+  unsigned long long n_eval = 0, n_write = 0, n_pass = 0;
   for (unsigned base = warp * 32; base < n; base += nwarp * 32) {
     const unsigned i = base + lane;
     if (i < n) {
@@ -641,23 +664,34 @@ __global__ void __launch_bounds__(32 * kQWarps) k_step(Fld64* fields, int nf, co
       const Fld64& F = fields[fi];
       const int slot = (int)(gid - F.gbase);
       atomicAnd(inq + (gid >> 5), ~(1u << (gid & 31)));   // listed again if moved meanwhile
-      const NewV nv = evaluate(F, slot);
-      ++n_eval;
-      if (nv.write) {
-        const double wend = __ldcg(F.clock);
-        if (nv.T < kReachD && nv.T > wend) {
-          push_id(q, gid);   // beyond the window: wait for it
-        } else {
+      const unsigned v0 = ld_ver(ver + gid);
+      const unsigned long long rec = __ldcg(pend + gid);
+      const double wend = __ldcg(F.clock);
+      if ((unsigned)(rec >> 32) == v0 && (double)__uint_as_float((unsigned)rec) > wend) {
+        push_id(q, gid);   // still beyond the window, inputs unchanged
+        ++n_pass;
+      } else {
+        const NewV nv = evaluate(F, slot);
+        ++n_eval;
+        if (nv.write) {
           const double oldT = F.T[slot];
-          F.T[slot] = nv.T;
-          F.G[slot] = make_double2(nv.gx, nv.gz);
-          F.fl[slot] = (uint8_t)((F.fl[slot] & kFlSeed) | (nv.copy ? kFlCopy : 0) |
-                                 (nv.sus ? kFlSusp : 0));
-          if (nv.spread) {
-            ++n_write;
-            F.clock[2] = 1.0;   // the window is not settled
-            __threadfence();
-            spread(F, q, slot, fmin(oldT, nv.T));
+          if (nv.T < kReachD && nv.T > wend) {
+            // beyond the window: wait for it (the time rounded down, so the
+            // compare above never passes over a node the window has reached)
+            pend[gid] = ((unsigned long long)v0 << 32) |
+                        (unsigned long long)__float_as_uint(__double2float_rd(nv.T));
+            push_id(q, gid);
+          } else {
+            F.T[slot] = nv.T;
+            F.G[slot] = make_double2(nv.gx, nv.gz);
+            F.fl[slot] = (uint8_t)((F.fl[slot] & kFlSeed) | (nv.copy ? kFlCopy : 0) |
+                                   (nv.sus ? kFlSusp : 0));
+            if (nv.spread) {
+              ++n_write;
+              F.clock[2] = 1.0;   // the window is not settled
+              __threadfence();
+              spread(F, q, slot, fmin(oldT, nv.T));
+            }
           }
         }
       }
@@ -668,10 +702,12 @@ __global__ void __launch_bounds__(32 * kQWarps) k_step(Fld64* fields, int nf, co
   for (int o = 16; o; o >>= 1) {
     n_eval += __shfl_xor_sync(0xffffffffu, n_eval, o);
     n_write += __shfl_xor_sync(0xffffffffu, n_write, o);
+    n_pass += __shfl_xor_sync(0xffffffffu, n_pass, o);
   }
-  if (lane == 0 && ctr && n_eval) {
+  if (lane == 0 && ctr && (n_eval || n_pass)) {
     atomicAdd(ctr + 0, n_eval);
     atomicAdd(ctr + 1, n_write);
+    atomicAdd(ctr + 2, n_pass);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -683,7 +719,6 @@ __global__ void __launch_bounds__(32 * kQWarps) k_step(Fld64* fields, int nf, co
     __threadfence();
     for (int f = threadIdx.x; f < nf; f += blockDim.x) {
       double* c = fields[f].clock;
-      // the window moves on only once nothing inside it changed in a step
       if (__ldcg(c + 2) == 0.0) c[0] = __ldcg(c) + __ldcg(c + 1);
       c[2] = 0.0;
     }
@@ -1104,9 +1139,10 @@ void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, unsigned*
   k_clock<<<nf, 256, 0, st>>>(f, nf, step);
 }
 void e64_step(Fld64* f, int nf, const unsigned* in, const unsigned* in_cnt, unsigned* out,
-              unsigned* out_cnt, unsigned* zero_cnt, unsigned* inq, unsigned* done, int grid,
-              unsigned long long* ctr, cudaStream_t st) {
-  k_step<<<grid, 32 * kQWarps, 0, st>>>(f, nf, in, in_cnt, out, out_cnt, zero_cnt, inq, done, ctr);
+              unsigned* out_cnt, unsigned* zero_cnt, unsigned* inq, unsigned* done, unsigned* ver,
+              unsigned long long* pend, int grid, unsigned long long* ctr, cudaStream_t st) {
+  k_step<<<grid, 32 * kQWarps, 0, st>>>(f, nf, in, in_cnt, out, out_cnt, zero_cnt, inq, done, ver,
+                                        pend, ctr);
 }
 void e64_verify(Fld64* f, int nf, size_t max_slots, unsigned* list, unsigned* cnt, unsigned* inq,
                 unsigned* bad, cudaStream_t st) {

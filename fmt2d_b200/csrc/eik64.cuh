@@ -63,9 +63,11 @@ void e64_seed_iface(Fld64* f, const Seed64* d, int nd, int nx, cudaStream_t st);
 // List every seeded node and its neighbours (list/cnt), set the windows.
 void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, unsigned* list,
                unsigned* cnt, unsigned* inq, cudaStream_t st);
+// One step over the list `in` (see k_step); ver / pend: per node input
+// version and deferred-time record, zeroed at the start of a batch.
 void e64_step(Fld64* f, int nf, const unsigned* in, const unsigned* in_cnt, unsigned* out,
-              unsigned* out_cnt, unsigned* zero_cnt, unsigned* inq, unsigned* done, int grid,
-              unsigned long long* ctr, cudaStream_t st);
+              unsigned* out_cnt, unsigned* zero_cnt, unsigned* inq, unsigned* done, unsigned* ver,
+              unsigned long long* pend, int grid, unsigned long long* ctr, cudaStream_t st);
 void e64_verify(Fld64* f, int nf, size_t max_slots, unsigned* list, unsigned* cnt, unsigned* inq,
                 unsigned* bad, cudaStream_t st);
 void e64_finish(Fld64* f, int nf, size_t max_slots, const int* water_up, cudaStream_t st);

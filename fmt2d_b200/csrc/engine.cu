@@ -282,8 +282,11 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   d_inq_.alloc(((total + 31) / 32) * sizeof(unsigned));
   d_count_.alloc(8 * sizeof(unsigned));
   d_done_.alloc(16);
-  d_ctr_.alloc(4 * sizeof(unsigned long long));
-  if (!d_list_.p || !d_inq_.p || !d_count_.p || !d_done_.p || !d_ctr_.p)
+  d_ctr_.alloc(8 * sizeof(unsigned long long));
+  d_ver_.alloc(total * sizeof(unsigned));
+  d_pend_.alloc(total * sizeof(unsigned long long));
+  if (!d_list_.p || !d_inq_.p || !d_count_.p || !d_done_.p || !d_ctr_.p || !d_ver_.p ||
+      !d_pend_.p)
     return "device allocation failed for the active lists";
   unsigned* L[3] = {d_list_.as<unsigned>(), d_list_.as<unsigned>() + total,
                     d_list_.as<unsigned>() + 2 * total};
@@ -292,7 +295,9 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   CK(cudaMemsetAsync(d_inq_.p, 0, ((total + 31) / 32) * sizeof(unsigned), stream_));
   CK(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned), stream_));
   CK(cudaMemsetAsync(d_done_.p, 0, 16, stream_));
-  CK(cudaMemsetAsync(dctr, 0, 4 * sizeof(unsigned long long), stream_));
+  CK(cudaMemsetAsync(dctr, 0, 8 * sizeof(unsigned long long), stream_));
+  CK(cudaMemsetAsync(d_ver_.p, 0, total * sizeof(unsigned), stream_));
+  CK(cudaMemsetAsync(d_pend_.p, 0, total * sizeof(unsigned long long), stream_));
   Fld64* dF = d_fields_.as<Fld64>();
   e64_fill(dF, nf, max_slots, stream_);
   ++stats_.launches;
@@ -344,7 +349,8 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   for (int k = 0; k < spc; ++k) {
     const int a = k % 3, b = (k + 1) % 3, c = (k + 2) % 3;
     e64_step(dF, nf, L[a], cnt + a, L[b], cnt + b, cnt + c, d_inq_.as<unsigned>(),
-             d_done_.as<unsigned>(), step_grid_, dctr, stream_);
+             d_done_.as<unsigned>(), d_ver_.as<unsigned>(), d_pend_.as<unsigned long long>(),
+             step_grid_, dctr, stream_);
   }
   CK(cudaMemcpyAsync(h_count_, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamEndCapture(stream_, &graph));
@@ -353,7 +359,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, stream_);
-  long long steps = 0;
+  long long steps = 0, steps_at_check = 0;
   int verify_passes = 0;
   std::string err;
   for (;;) {
@@ -363,8 +369,16 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     stats_.launches += spc;
     const cudaError_t se = cudaStreamSynchronize(stream_);
     if (se != cudaSuccess) { err = std::string("step loop: ") + cudaGetErrorString(se); break; }
-    if (steps >= max_steps) { err = "eikonal solve did not converge within the step cap"; break; }
-    if (h_count_[0] != 0u) continue;
+    if (h_count_[0] != 0u) {
+      // after a fixed-point check no node is final, so what still moves
+      // gets a bounded number of steps and is reported in the stats
+      if (verify_passes > 0 && steps - steps_at_check >= check_steps) {
+        stats_.capped += h_count_[0];
+        break;
+      }
+      if (steps >= max_steps) { err = "eikonal solve did not converge within the step cap"; break; }
+      continue;
+    }
     // empty list: check the fixed point of every node, resume if needed
     if (verify_passes >= 6) break;   // nodes still moving are reported in the stats
     ++verify_passes;
@@ -375,8 +389,9 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     cudaMemcpyAsync(h_count_, cnt + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_);
     const cudaError_t ve = cudaStreamSynchronize(stream_);
     if (ve != cudaSuccess) { err = std::string("fixed-point check: ") + cudaGetErrorString(ve); break; }
-    stats_.capped = h_count_[0];
+    steps_at_check = steps;
     if (h_count_[0] == 0u) break;
+    stats_.unsettled = h_count_[0];
   }
   cudaEventRecord(e1, stream_);
   cudaEventSynchronize(e1);
@@ -388,13 +403,14 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   cudaGraphDestroy(graph);
   if (!err.empty()) return err;
   stats_.round_ms += ms;
-  stats_.rounds += (int)steps;
+  stats_.rounds += steps;
   {
-    unsigned long long c[4];
+    unsigned long long c[3];
     CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
-    stats_.updates += c[0];
-    stats_.passes += c[1];
-    stats_.steps += steps / spc;
+    stats_.evals += c[0];
+    stats_.writes += c[1];
+    stats_.passed += c[2];
+    stats_.graphs += steps / spc;
   }
   e64_finish(dF, nf, max_slots, d_up_.as<int>(), stream_);
   stats_.launches += 2;

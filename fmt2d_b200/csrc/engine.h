@@ -44,11 +44,13 @@ struct FieldStore {
 };
 
 struct SolveStats {
-  int rounds = 0, batches = 0, final_passes = 0;
-  long long tile_visits = 0;
-  double round_ms = 0.0;     // device time of the step kernels
-  // node evaluations, writes, graph launches
-  unsigned long long passes = 0, steps = 0, capped = 0, updates = 0;
+  long long rounds = 0;       // step kernels run
+  int batches = 0, final_passes = 0;   // stage batches; fixed-point checks
+  double round_ms = 0.0;      // device time of the step loops
+  unsigned long long evals = 0, writes = 0, passed = 0;   // node evaluations; writes; deferred nodes passed over
+  unsigned long long graphs = 0;      // captured step graphs launched
+  unsigned long long unsettled = 0;   // nodes the last fixed-point check re-listed
+  unsigned long long capped = 0;      // nodes still moving when the steps after a check ran out
   long long launches = 0;     // kernels launched since the last forward began
   long long nodes = 0;        // region nodes of the time fields solved
 };
@@ -75,9 +77,10 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
   const SolveStats& stats() const { return stats_; }
   int inner = 1;             // unused by the list schedule (kept for the C ABI)
-  double window_cells = 4.0; // window step: this many cells at the region's largest velocity
+  double window_cells = 0.5; // window step: this many cells at the region's largest velocity
   int steps_per_check = 24;  // steps per captured graph between list checks (multiple of 3)
-  long long max_steps = 200000;   // safety cap on steps per level
+  long long max_steps = 2000000;  // safety cap on steps per level
+  long long check_steps = 4096;   // steps allowed after each fixed-point check
   // device pointers of a solved field (FP64 time, double2 final gradient per slot)
   const double* field_t(int src, int tf) const { return fields_[src][tf].T.as<double>(); }
   const double2* field_g(int src, int tf) const { return fields_[src][tf].Gout.as<double2>(); }
@@ -101,7 +104,7 @@ class Engine {
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
   DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_count_, d_scratch_, d_which_, d_up_, d_step_,
-      d_done_, d_ctr_, d_list_, d_inq_;
+      d_done_, d_ctr_, d_list_, d_inq_, d_ver_, d_pend_;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
       d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
   int npick_ = -1, rows_ = 0;

@@ -102,12 +102,15 @@ FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int p
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
 /* Counters of the last fmt2d_forward (and of the exports since), in this
- * order: [0] relaxation rounds, [1] stage batches, [2] final gradient passes,
- * [3] tile visits, [4] device milliseconds of the relaxation kernel, [5] kernel
- * launches, [6] region nodes of the solved time fields, [7] sweep passes,
- * [8] warp sweep steps, [9] visits that hit the pass cap, [10] node updates.
+ * order: [0] step kernels, [1] stage batches, [2] fixed-point checks,
+ * [3] deferred nodes passed over without evaluation, [4] device milliseconds
+ * of the step loops, [5] kernel launches, [6] region nodes of the solved time
+ * fields, [7] node evaluations, [8] step graphs launched, [9] nodes still
+ * moving when the steps allowed after a fixed-point check ran out (0 when
+ * every field reached its fixed point), [10] node writes, [11] nodes the
+ * last fixed-point check re-listed.
  * Writes min(n, FMT2D_N_STATS) values.  No reference counterpart (diagnostics). */
-#define FMT2D_N_STATS 11
+#define FMT2D_N_STATS 12
 FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
 
 /* Ray backtrace and Frechet rows of npick picks on the fields of the last
@@ -186,9 +189,12 @@ FMT2D_API int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params
 FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* Schedule of the eikonal solve (no reference counterpart; the reference's
- * heap has no schedule): relaxation rounds per tile visit (1..64), the time
- * window's step in cells at the region's largest velocity (> 0), and steps
- * between convergence checks (1..256).  Results do not depend on them. */
+ * heap has no schedule): `inner` is accepted for compatibility and unused
+ * (1..64), the time window's step in cells at the region's largest velocity
+ * (> 0, default 0.5), and steps between convergence checks (1..256).  The
+ * window bounds how far ahead of the settled times a node may be written:
+ * wider windows reach fixed points that can differ from the heap's order and
+ * take more steps per window; the default is the one the parity tests use. */
 FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, int inner, double window_cells,
                                  int steps_per_check);
 
