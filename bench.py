@@ -12,9 +12,10 @@ eikonal time fields, solved through the library's public entry point.
 * e2e    : the same metric through the public API from host buffers: model
            upload (host arrays -> device), the forward solve, and the read-back
            of every terminal-stage traveltime field to host memory.
-* roofline: the relaxation kernel against the measured HBM bandwidth, with the
-           algorithmic traffic of one field (16 B per region node: time and
-           gradient written once, velocity and geometry code read once).
+* roofline: the step kernel (k_step) against the measured HBM bandwidth, with
+           the algorithmic traffic of one field: 36 B per region node (FP64
+           time and gradient written once, FP64 velocity and the 4-byte node
+           code read once), over the device time of the step loops.
 * cpu_baseline: the FP64 CPU restatement of the reference algorithm (oracle/)
            on the host cores, over a bounded sample of the same workload.
 * --impl reference: the CPU restatement timed on all host cores (the reference
@@ -309,11 +310,11 @@ def run_ours(args, world, rank, local):
     if rank != 0:
         return
     peak, peak_kind = measured_peak_hbm()
-    alg_bytes = 16.0 * nodes / args.steps          # per step, all fields
+    alg_bytes = 36.0 * nodes / args.steps          # per step, all fields
     achieved = alg_bytes / (solve_ms / args.steps / 1e3) / 1e9 if solve_ms > 0 else None
     out = {"metric": METRIC, "value": round(value, 3), "unit": "fields/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 3),
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
            "config": {"workload": WORKLOAD, "grid": "2001x401", "sources_per_gpu": int(src.size),
                       "fields_per_gpu": nf, "l2": "field data per step (> 1 GB) exceeds L2",
@@ -321,7 +322,7 @@ def run_ours(args, world, rank, local):
            "e2e": {"value": round(e2e_value, 3), "unit": "fields/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(d2h), "includes": "model upload, forward, "
                    "terminal-stage traveltime read-back"},
-           "roofline": {"bound": "hbm", "kernel": "eik_visit",
+           "roofline": {"bound": "hbm", "kernel": "k_step",
                         "achieved": round(achieved, 3) if achieved else None,
                         "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 6) if achieved else None,
