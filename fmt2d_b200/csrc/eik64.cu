@@ -514,6 +514,16 @@ __device__ __forceinline__ unsigned ld_ver(const unsigned* p) {
   return v;
 }
 
+// Append a node that this thread has just marked queued.
+__device__ __forceinline__ void stage_id(const Queue& q, unsigned gid) {
+  const unsigned p = atomicAdd(q.scnt, 1u);
+  if (p < (unsigned)kQBuf) {
+    q.sbuf[p] = gid;
+  } else {
+    q.out[atomicAdd(q.out_cnt, 1u)] = gid;
+  }
+}
+
 __device__ __forceinline__ void push_id(const Queue& q, unsigned gid) {
   const unsigned bit = 1u << (gid & 31);
   if (atomicOr(q.inq + (gid >> 5), bit) & bit) return;   // already queued
@@ -567,24 +577,68 @@ __device__ __forceinline__ void queue_iface(const Fld64& F, const Queue& q, int 
 // diagonal neighbours, and the interface nodes of the cut cells it is a
 // corner of.
 __device__ void spread_grid(const Fld64& F, const Queue& q, int r, int c, double thr) {
-  queue_grid(F, q, r - 2, c, thr);
-  queue_grid(F, q, r + 2, c, thr);
-  queue_grid(F, q, r, c - 2, thr);
-  queue_grid(F, q, r, c + 2, thr);
+  // The targets' loads and atomics are issued in batches (independent of one
+  // another), so the latency is paid a few times instead of once per target.
+  // Grid targets: the second neighbours along the axes and the 3x3 block.
+  constexpr int kN = 12;
+  const int dr[kN] = {-2, 2, 0, 0, -1, -1, -1, 0, 0, 1, 1, 1};
+  const int dc[kN] = {0, 0, -2, 2, -1, 0, 1, -1, 1, -1, 0, 1};
+  int sl[kN];
+  bool ok[kN];
 #pragma unroll
-  for (int dr = -1; dr <= 1; ++dr)
+  for (int k = 0; k < kN; ++k) {
+    const int rr = r + dr[k], cc = c + dc[k];
+    ok[k] = rr >= 0 && rr < F.H && cc >= 0 && cc < F.nx;
+    sl[k] = ok[k] ? rr * F.pitch + cc : 0;
+  }
+  uint32_t code[kN];
 #pragma unroll
-    for (int dc = -1; dc <= 1; ++dc)
-      if (dr || dc) queue_grid(F, q, r + dr, c + dc, thr);
+  for (int k = 0; k < kN; ++k) code[k] = ok[k] ? __ldg(F.code + sl[k]) : 0u;
+#pragma unroll
+  for (int k = 0; k < kN; ++k) ok[k] = ok[k] && (code[k] & kInRegion);
+  double tv[kN];
+#pragma unroll
+  for (int k = 0; k < kN; ++k) tv[k] = ok[k] ? ldT(F, sl[k]) : 0.0;
+  if (q.ver) {
+#pragma unroll
+    for (int k = 0; k < kN; ++k)
+      if (ok[k]) atomicAdd(q.ver + F.gbase + sl[k], 1u);
+  }
+  unsigned was[kN];
+#pragma unroll
+  for (int k = 0; k < kN; ++k) {
+    ok[k] = ok[k] && !(tv[k] < thr);
+    const unsigned gid = F.gbase + (unsigned)sl[k];
+    was[k] = ok[k] ? atomicOr(q.inq + (gid >> 5), 1u << (gid & 31)) : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < kN; ++k) {
+    const unsigned gid = F.gbase + (unsigned)sl[k];
+    if (ok[k] && !(was[k] & (1u << (gid & 31)))) stage_id(q, gid);
+  }
+  // interface nodes of the cut cells (r, c) is a corner of
   const int ar = F.z_lo + r;
+  int isl[4];
+  bool iok[4];
 #pragma unroll
-  for (int side = 0; side < 2; ++side)
+  for (int k = 0; k < 4; ++k) {
+    const int side = k >> 1, kc = c - 1 + (k & 1);
+    iok[k] = kc >= 0 && kc < F.nx;
+    const int izc = iok[k] ? __ldg(F.izc + side * F.pitch + kc) : -1;
+    iok[k] = iok[k] && izc >= 0 && (izc == ar || izc + 1 == ar);
+    isl[k] = iok[k] ? (F.H + side) * F.pitch + kc : 0;
+  }
+  double itv[4];
 #pragma unroll
-    for (int k = c - 1; k <= c; ++k) {
-      if (k < 0 || k >= F.nx) continue;
-      const int izc = __ldg(F.izc + side * F.pitch + k);
-      if (izc >= 0 && (izc == ar || izc + 1 == ar)) queue_iface(F, q, side, k, thr);
-    }
+  for (int k = 0; k < 4; ++k) itv[k] = iok[k] ? ldT(F, isl[k]) : 0.0;
+  if (q.ver) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (iok[k]) atomicAdd(q.ver + F.gbase + isl[k], 1u);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (iok[k] && !(itv[k] < thr)) push_id(q, F.gbase + (unsigned)isl[k]);
 }
 
 __device__ void spread_iface(const Fld64& F, const Queue& q, int side, int c, double thr) {
