@@ -78,38 +78,73 @@ struct RNb {
   double T, T2, d2, dpos;
 };
 
-// Neighbour (r+dr, c+dc) of the grid node (r, c) with velocity vu: reached,
+// The direct neighbour of a grid node as regular_update2d sees it: reached,
 // the face velocity term and the second-order switch (:642-673, :688-719).
-__device__ void rnb(const Fld64& F, int r, int c, int dr, int dc, double vu, RNb& n) {
-  n.ok = false;
-  n.second = false;
-  n.dirx = dc != 0;
-  const int rn = r + dr, cn = c + dc;
-  if (rn < 0 || rn >= F.H || cn < 0 || cn >= F.nx) return;
-  const int sn = rn * F.pitch + cn;
-  if (!(__ldg(F.code + sn) & kInRegion)) return;
-  const double Tn = ldT(F, sn);
-  if (!(Tn < kReachD)) return;
-  const double vn = __ldg(F.vel + sn);
-  n.ok = true;
-  n.single_ok = sn != F.frozen_slot;
-  n.T = Tn;
-  const double velx = 0.5 * (vu + vn);
-  const double dd = velx / F.dx;
-  n.d2 = dd * dd;
-  n.dpos = n.dirx ? xg(F, c) - xg(F, cn) : zg(F, r) - zg(F, rn);
-  const int r2 = r + 2 * dr, c2 = c + 2 * dc;
-  if (r2 < 0 || r2 >= F.H || c2 < 0 || c2 >= F.nx) return;
-  const int s2 = r2 * F.pitch + c2;
-  if (!(__ldg(F.code + s2) & kInRegion)) return;
-  const double T2 = ldT(F, s2);
-  if (!(T2 < kReachD) || !(Tn >= T2)) return;
-  const double v2 = __ldg(F.vel + s2);
-  if (!(vn * v2 > kTinyD)) return;
-  const double2 gn = ldG(F, sn), g2 = ldG(F, s2);
-  if (gn.x * g2.x + gn.y * g2.y >= 0.71 / (vn * v2)) {
-    n.second = true;
-    n.T2 = T2;
+// The four direct neighbours (L, R, U, D) at once, with the loads of all four
+// directions issued together (codes, then times and velocities, then the
+// gradients the second-order switch needs), so a node pays a few memory round
+// trips instead of a chain per direction.
+__device__ void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
+  const int dr[4] = {0, 0, -1, 1}, dc[4] = {-1, 1, 0, 0};
+  int s1[4], s2[4];
+  bool b1[4], b2[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int rn = r + dr[k], cn = c + dc[k], r2 = r + 2 * dr[k], c2 = c + 2 * dc[k];
+    b1[k] = rn >= 0 && rn < F.H && cn >= 0 && cn < F.nx;
+    b2[k] = b1[k] && r2 >= 0 && r2 < F.H && c2 >= 0 && c2 < F.nx;
+    s1[k] = b1[k] ? rn * F.pitch + cn : 0;
+    s2[k] = b2[k] ? r2 * F.pitch + c2 : 0;
+  }
+  uint32_t k1[4], k2[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    k1[k] = b1[k] ? __ldg(F.code + s1[k]) : 0u;
+    k2[k] = b2[k] ? __ldg(F.code + s2[k]) : 0u;
+  }
+  double t1[4], t2[4], v1[4], v2[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    b1[k] = b1[k] && (k1[k] & kInRegion);
+    b2[k] = b2[k] && (k2[k] & kInRegion);
+    t1[k] = b1[k] ? ldT(F, s1[k]) : kHugeD;
+    v1[k] = b1[k] ? __ldg(F.vel + s1[k]) : 0.0;
+    t2[k] = b2[k] ? ldT(F, s2[k]) : kHugeD;
+    v2[k] = b2[k] ? __ldg(F.vel + s2[k]) : 0.0;
+  }
+  bool need[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    RNb& m = n[k];
+    m.ok = false;
+    m.second = false;
+    m.dirx = dc[k] != 0;
+    need[k] = false;
+    if (!b1[k] || !(t1[k] < kReachD)) continue;
+    m.ok = true;
+    m.single_ok = s1[k] != F.frozen_slot;
+    m.T = t1[k];
+    const double velx = 0.5 * (vu + v1[k]);
+    const double dd = velx / F.dx;
+    m.d2 = dd * dd;
+    m.dpos = m.dirx ? xg(F, c) - xg(F, c + dc[k]) : zg(F, r) - zg(F, r + dr[k]);
+    if (!b2[k]) continue;
+    if (!(t2[k] < kReachD) || !(t1[k] >= t2[k])) continue;
+    if (!(v1[k] * v2[k] > kTinyD)) continue;
+    need[k] = true;
+  }
+  double2 g1[4], g2[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    g1[k] = need[k] ? ldG(F, s1[k]) : make_double2(0.0, 0.0);
+    g2[k] = need[k] ? ldG(F, s2[k]) : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (need[k] && g1[k].x * g2[k].x + g1[k].y * g2[k].y >= 0.71 / (v1[k] * v2[k])) {
+      n[k].second = true;
+      n[k].T2 = t2[k];
+    }
   }
 }
 
@@ -410,11 +445,9 @@ __device__ NewV update_grid(const Fld64& F, int r, int c) {
   const uint32_t code = __ldg(F.code + s);
   if (!(code & kInRegion) || !(code & kUpdatable) || s == F.frozen_slot) return none;
   const double vu = __ldg(F.vel + s);
-  RNb L, R, U, D;
-  rnb(F, r, c, 0, -1, vu, L);
-  rnb(F, r, c, 0, +1, vu, R);
-  rnb(F, r, c, -1, 0, vu, U);
-  rnb(F, r, c, +1, 0, vu, D);
+  RNb nb[4];
+  rnb4(F, r, c, vu, nb);
+  const RNb &L = nb[0], &R = nb[1], &U = nb[2], &D = nb[3];
   if (code & kFullyRegular) {
     // update_time2d's quadrant loop: (L,U), (R,U), (L,D), (R,D)
     Cand best = no_cand();
