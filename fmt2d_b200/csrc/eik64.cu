@@ -78,12 +78,11 @@ struct RNb {
   double T, T2, d2, dpos;
 };
 
-// The direct neighbour of a grid node as regular_update2d sees it: reached,
-// the face velocity term and the second-order switch (:642-673, :688-719).
-// The four direct neighbours (L, R, U, D) at once, with the loads of all four
-// directions issued together (codes, then times and velocities, then the
-// gradients the second-order switch needs), so a node pays a few memory round
-// trips instead of a chain per direction.
+// The four direct neighbours (L, R, U, D) of grid node (r, c): reached, the
+// face velocity term and the second-order switch (:642-673, :688-719), with
+// the loads of all four directions issued together (codes, then times and
+// velocities, then the gradients the switch needs), so a node pays a few
+// memory round trips instead of a chain per direction.
 __device__ void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
   const int dr[4] = {0, 0, -1, 1}, dc[4] = {-1, 1, 0, 0};
   int s1[4], s2[4];
