@@ -162,13 +162,18 @@ def measured_peak_hbm():
 
 
 def dist_setup(n_gpus):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL
+    when a CUDA device is present, gloo otherwise (host-only runs and tests).
+    Only the timing is reduced across ranks: the sources are independent."""
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local = _env_int("LOCAL_RANK", 0)
     if world > 1:
-        import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
