@@ -202,6 +202,32 @@ class Fmt2d:
                     "fmt2d_lsqr")
         return dm, it.value, rn.value, bn.value, t2.value
 
+    def lsqr_damped(self, residual, dm_sum=None, gtg_diag=None, mvscale=None, *,
+                    lam_damp=0.0, lam_damp_iface=0.0, target_dv=0.0, target_dd=0.0,
+                    w_smooth=0.0, w_smooth_iface=0.0, eps_min=0.0, max_iter=2000):
+        """lsqr_inversion2d's damping choice (src/inversion2d.f90:533-739):
+        a fixed damping weight (lam_damp > 0) or tomo2d's auto damping towards
+        the RMS velocity change target_dv and depth change target_dd, each
+        solve an fmt2d_lsqr on the current G.  mvscale (column scaling, for
+        the depth change of interface parameters) defaults to ones and gtg_diag
+        to this G's column norms.  Returns a damping.DampingResult."""
+        from .damping import damping_search
+        if gtg_diag is None:
+            gtg_diag = self.gtg_diag()
+        gtg_diag = np.ascontiguousarray(gtg_diag, dtype=np.float64)
+        if mvscale is None:
+            mvscale = np.ones(self.nparm)
+        _, nvp, _ = self.inv_index()
+
+        def solve(wdv, wdi):
+            return self.lsqr(residual, dm_sum, gtg_diag, wdv=wdv, wdv_iface=wdi,
+                             w_smooth=w_smooth, w_smooth_iface=w_smooth_iface,
+                             eps_min=eps_min, max_iter=max_iter)[0]
+
+        return damping_search(solve, dm_sum, gtg_diag, mvscale, eps_min, nvp,
+                              lam_damp=lam_damp, lam_damp_iface=lam_damp_iface,
+                              target_dv=target_dv, target_dd=target_dd)
+
     def lsqr_stats(self):
         ms, n = C.c_double(), C.c_int()
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
