@@ -67,6 +67,9 @@ def lib():
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
     L.fmt2d_set_schedule.argtypes = [V, C.c_int, C.c_double, C.c_int]
+    L.fmt2d_gauss_smooth.argtypes = [V, C.c_int, C.c_double, C.c_double, C.c_double,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     P(C.c_longlong)]
     L.fmt2d_trace.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, P(C.c_longlong)]
     L.fmt2d_frechet_rows.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]

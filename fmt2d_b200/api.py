@@ -110,6 +110,25 @@ class Fmt2d:
                     "fmt2d_inv_index")
         return out.reshape(self.nz, self.nx), nvp.value, npar.value
 
+    def gauss_smooth(self, which: int, mvscale, corr_x=0.0, corr_z=0.0, corr_x_iface=0.0):
+        """1-based CSR (row_ptr, col, val) of the Gaussian smoothing matrix R_h
+        (which 0), R_v (1) or the interface R_h (2) (fmt2d_gauss_smooth)."""
+        mv = np.ascontiguousarray(mvscale, dtype=np.float64)
+        npar = self.inv_index()[2]
+        if mv.size != npar:
+            raise ValueError(f"mvscale has {mv.size} entries, the model has {npar} parameters")
+        nnz = C.c_longlong()
+        self._check(self.L.fmt2d_gauss_smooth(self.h, int(which), float(corr_x), float(corr_z),
+                                              float(corr_x_iface), N.ptr(mv), None, None, None,
+                                              C.byref(nnz)), "fmt2d_gauss_smooth")
+        rp = np.zeros(mv.size + 1, np.int32)
+        col, val = np.zeros(max(nnz.value, 1), np.int32), np.zeros(max(nnz.value, 1))
+        self._check(self.L.fmt2d_gauss_smooth(self.h, int(which), float(corr_x), float(corr_z),
+                                              float(corr_x_iface), N.ptr(mv), N.ptr(rp),
+                                              N.ptr(col), N.ptr(val), C.byref(nnz)),
+                    "fmt2d_gauss_smooth")
+        return rp, col[:nnz.value], val[:nnz.value]
+
     def forward(self, src_x, phases=(1, 2, 3, 4, 5)):
         src_x = np.ascontiguousarray(src_x, dtype=np.float64)
         self.mask = phase_mask(phases)

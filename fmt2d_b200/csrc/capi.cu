@@ -137,6 +137,23 @@ int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, double* z, doub
   return FMT2D_OK;
 }
 
+int fmt2d_gauss_smooth(fmt2d_ctx* ctx, int which, double corr_x, double corr_z,
+                       double corr_x_iface, const double* mvscale, int* row_ptr, int* col,
+                       double* val, long long* nnz) {
+  if (!ctx || !mvscale || !nnz || which < 0 || which > 2) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  std::vector<int> rp, c;
+  std::vector<double> v;
+  const std::string e = fmt2d::gauss_smooth_csr(ctx->model, which, corr_x, corr_z, corr_x_iface,
+                                                mvscale, rp, c, v);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  *nnz = (long long)c.size();
+  if (row_ptr) std::copy(rp.begin(), rp.end(), row_ptr);
+  if (col) std::copy(c.begin(), c.end(), col);
+  if (val) std::copy(v.begin(), v.end(), val);
+  return FMT2D_OK;
+}
+
 int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* nvp, int* npar) {
   if (!ctx) return FMT2D_ERR_ARG;
   if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");

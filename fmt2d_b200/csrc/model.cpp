@@ -318,4 +318,92 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
   return std::string();
 }
 
+namespace {
+
+// One Gaussian row: exp(-d^2 / c^2) * mvscale(j) for the listed neighbours j
+// of parameter i in the given order, then the diagonal -sum * mvscale(i).
+struct GaussRow {
+  std::vector<int> col;
+  std::vector<double> val;
+  double bsum = 0.0;
+  void add(int j, double d, double c, const double* mvscale) {
+    const double beta = std::exp(-(d * d) / (c * c));
+    bsum = bsum + beta;
+    col.push_back(j);
+    val.push_back(beta * mvscale[j - 1]);
+  }
+  void close(int i, const double* mvscale) {
+    col.push_back(i);
+    val.push_back(-bsum * mvscale[i - 1]);
+  }
+};
+
+}  // namespace
+
+std::string gauss_smooth_csr(const Model& m, int which, double corr_x, double corr_z,
+                             double corr_x_iface, const double* mvscale, std::vector<int>& rp,
+                             std::vector<int>& col, std::vector<double>& val) {
+  const int np = m.n_inv_parms;
+  std::vector<GaussRow> rows(np + 1);
+  if (which == 0 || which == 1) {
+    if (which == 0 && !(corr_x > 0.0)) return "corr_x must be > 0";
+    if (which == 1 && !(corr_z > 0.0)) return "corr_z must be > 0";
+    // R_h: neighbours along the grid row within int(3 cx / dx) + 1 columns;
+    // R_v: along the grid column within 3 cz (build_gauss_smooth_matrix)
+    const int reach = (int)(3.0 * corr_x / m.dx) + 1;
+    for (int iz = 0; iz < m.nz; ++iz)
+      for (int ix = 0; ix < m.nx; ++ix) {
+        const int i = m.inv_idx[m.g(ix, iz)];
+        if (i <= 0) continue;
+        GaussRow& R = rows[i];
+        if (which == 0) {
+          const int lo = std::max(0, ix - reach), hi = std::min(m.nx - 1, ix + reach);
+          for (int jx = lo; jx <= hi; ++jx) {
+            const int j = jx == ix ? 0 : m.inv_idx[m.g(jx, iz)];
+            if (j > 0) R.add(j, grid_x(m, jx) - grid_x(m, ix), corr_x, mvscale);
+          }
+        } else {
+          for (int jz = 0; jz < m.nz; ++jz) {
+            if (jz == iz) continue;
+            const double d = grid_z(m, jz) - grid_z(m, iz);
+            if (std::fabs(d) > 3.0 * corr_z) continue;
+            const int j = m.inv_idx[m.g(ix, jz)];
+            if (j > 0) R.add(j, d, corr_z, mvscale);
+          }
+        }
+        R.close(i, mvscale);
+      }
+  } else if (which == 2) {
+    // interface R_h over the inverted interface's nodes (parameters
+    // n_vel_parms + 1 ..), build_iface_gauss_smooth_matrix; none when the
+    // correlation length is 0 or no interface is inverted
+    if (corr_x_iface > 0.0 && m.iface_inv > 0) {
+      const double dx_if = m.xpos[1] - m.xpos[0];
+      const int reach = (int)(3.0 * corr_x_iface / dx_if) + 1;
+      for (int ix = 0; ix < m.nx; ++ix) {
+        const int i = m.n_vel_parms + ix + 1;
+        if (i < 1 || i > np) continue;
+        GaussRow& R = rows[i];
+        const int lo = std::max(0, ix - reach), hi = std::min(m.nx - 1, ix + reach);
+        for (int jx = lo; jx <= hi; ++jx) {
+          const int j = m.n_vel_parms + jx + 1;
+          if (jx != ix && j >= 1 && j <= np) R.add(j, m.xpos[jx] - m.xpos[ix], corr_x_iface, mvscale);
+        }
+        R.close(i, mvscale);
+      }
+    }
+  } else {
+    return "which must be 0 (R_h), 1 (R_v) or 2 (interface R_h)";
+  }
+  rp.assign(np + 1, 1);
+  col.clear();
+  val.clear();
+  for (int i = 1; i <= np; ++i) {
+    col.insert(col.end(), rows[i].col.begin(), rows[i].col.end());
+    val.insert(val.end(), rows[i].val.begin(), rows[i].val.end());
+    rp[i] = (int)col.size() + 1;
+  }
+  return std::string();
+}
+
 }  // namespace fmt2d

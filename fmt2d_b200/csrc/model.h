@@ -95,4 +95,14 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
                         const double* zrel, const double* vel, double vwater,
                         const double* sed_z, const double* moho_z, int iface_inv);
 
+// Gaussian smoothing matrix of the smooth_type 2/3 LSQR layouts as 1-based
+// CSR over all n_inv_parms rows (rows it does not cover stay empty), mvscale
+// folded into the values: which 0 = R_h, 1 = R_v over the velocity
+// parameters (build_gauss_smooth_matrix, src/inversion2d.f90:1252-1402),
+// 2 = R_h over the inverted interface (build_iface_gauss_smooth_matrix,
+// :1524-1616).  Returns an error message or "".
+std::string gauss_smooth_csr(const Model& m, int which, double corr_x, double corr_z,
+                             double corr_x_iface, const double* mvscale, std::vector<int>& rp,
+                             std::vector<int>& col, std::vector<double>& val);
+
 }  // namespace fmt2d

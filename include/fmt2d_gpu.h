@@ -95,6 +95,19 @@ FMT2D_API int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, doubl
  * fastest, 1-based ids, 0 inactive; returns counts. */
 FMT2D_API int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* n_vel_parms, int* n_inv_parms);
 
+/* Gaussian smoothing matrix of run_lsqr's smooth_type 2/3 layouts, built on
+ * the host (works on a host-only context): which 0 = R_h and 1 = R_v over the
+ * velocity parameters (build_gauss_smooth_matrix, src/inversion2d.f90:
+ * 1252-1402), 2 = R_h over the inverted interface's parameters
+ * (build_iface_gauss_smooth_matrix, :1524-1616); correlation lengths in km,
+ * mvscale[n_inv_parms] folded into the values as the reference does.  1-based
+ * CSR over all n_inv_parms rows, rows the matrix does not cover empty:
+ * row_ptr[n_inv_parms + 1], col[nnz], val[nnz]; call with col = val = NULL
+ * to get *nnz first. */
+FMT2D_API int fmt2d_gauss_smooth(fmt2d_ctx* ctx, int which, double corr_x, double corr_z,
+                                 double corr_x_iface, const double* mvscale, int* row_ptr,
+                                 int* col, double* val, long long* nnz);
+
 /* Solve every time field of the enabled phases (bit p-1 of phase_mask enables
  * phase p) for nsrc OBS sources placed on the seafloor below src_x[s]. */
 FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask);

@@ -67,6 +67,11 @@ int orc_lsqr(void* h, int ndata, int nparm, const int* gindx, const double* gval
 void orc_spmv(int ndata, int nparm, const int* gindx, const double* gval, const int* row_ptr,
               int transpose, const double* x, double* y);
 void orc_laplacian(void* h, int nparm, const double* vin, double* vout);
+/* Gaussian smoothing matrices of build_gauss_smooth_matrix (which 0: R_h,
+ * 1: R_v) and build_iface_gauss_smooth_matrix (which 2), inversion2d.f90:
+ * 1252-1616, as 1-based CSR over the model's parameters; returns nnz. */
+int orc_gauss_smooth(void* h, double corr_x, double corr_z, double corr_x_iface,
+                     const double* mvscale, int which, int* rp, int* col, double* val, int cap);
 
 #ifdef __cplusplus
 }

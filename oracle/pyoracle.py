@@ -71,6 +71,9 @@ def lib():
                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.orc_spmv.argtypes = [C.c_int, C.c_int, _ip, _dp, _ip, C.c_int, _dp, _dp]
     L.orc_laplacian.argtypes = [V, C.c_int, _dp, _dp]
+    L.orc_gauss_smooth.restype = C.c_int
+    L.orc_gauss_smooth.argtypes = [V, C.c_double, C.c_double, C.c_double, _dp, C.c_int,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     _lib = L
     return L
 
@@ -184,6 +187,20 @@ class Oracle:
                        f64(gtg), f64(dm_sum), eps_min, wdv, wdv_iface, w_smooth, w_smooth_iface,
                        max_iter, dm, C.byref(it), C.byref(rn), C.byref(t2))
         return dm, it.value, rn.value, t2.value
+
+    def gauss_smooth(self, which, mvscale, corr_x=0.0, corr_z=0.0, corr_x_iface=0.0):
+        """1-based CSR (rp, col, val) of R_h (which 0), R_v (1) or the
+        interface R_h (2) of build_gauss_smooth_matrix /
+        build_iface_gauss_smooth_matrix."""
+        mv = np.ascontiguousarray(mvscale, dtype=np.float64)
+        rp = np.zeros(mv.size + 1, np.int32)
+        n = lib().orc_gauss_smooth(self.h, corr_x, corr_z, corr_x_iface, mv, which, None, None,
+                                   None, 0)
+        col, val = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1))
+        lib().orc_gauss_smooth(self.h, corr_x, corr_z, corr_x_iface, mv, which,
+                               rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                               val.ctypes.data_as(C.c_void_p), n)
+        return rp, col[:n], val[:n]
 
     def laplacian(self, nparm, v):
         out = np.zeros(nparm)

@@ -2,6 +2,7 @@
 #include "../fmt2d_oracle.h"
 #include "oracle.hpp"
 #include "lsqr.hpp"
+#include "smooth.hpp"
 #include <map>
 #include <memory>
 #include <algorithm>
@@ -258,6 +259,23 @@ void orc_laplacian(void* h, int nparm, const double* vin, double* vout) {
   G.nx = m.grid.nx; G.nz = m.grid.nz; G.inv_idx = m.inv_idx.data();
   if (m.iface_inv > 0) { G.iface_start = m.iface_start; G.iface_nx = m.isec[m.iface_inv].nnode; }
   orc::laplacian(G, nparm, vin, vout);
+}
+
+// Gaussian smoothing matrices: which 0 = R_h, 1 = R_v (velocity parameters),
+// 2 = interface R_h.  Writes the 1-based CSR (rp[nparm+1], col/val up to cap)
+// and returns nnz.
+int orc_gauss_smooth(void* h, double corr_x, double corr_z, double corr_x_iface,
+                     const double* mvscale, int which, int* rp, int* col, double* val, int cap) {
+  const orc::Model& m = H(h)->m;
+  const int nparm = m.n_inv_parms;
+  orc::Csr a, b;
+  if (which == 2) orc::iface_gauss_smooth_matrix(m, nparm, corr_x_iface, mvscale, a);
+  else orc::gauss_smooth_matrices(m, nparm, corr_x, corr_z, mvscale, a, b);
+  const orc::Csr& r = which == 1 ? b : a;
+  const int nnz = (int)r.col.size();
+  if (rp) std::copy(r.rp.begin(), r.rp.end(), rp);
+  for (int k = 0; k < nnz && k < cap; ++k) { col[k] = r.col[k]; val[k] = r.val[k]; }
+  return nnz;
 }
 
 }  // extern "C"
