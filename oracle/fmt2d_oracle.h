@@ -67,6 +67,14 @@ int orc_lsqr(void* h, int ndata, int nparm, const int* gindx, const double* gval
 void orc_spmv(int ndata, int nparm, const int* gindx, const double* gval, const int* row_ptr,
               int transpose, const double* x, double* y);
 void orc_laplacian(void* h, int nparm, const double* vin, double* vout);
+/* run_lsqr for smooth_type 1 (Laplacian), 2 (Gaussian R_h, R_v) or 3 (Laplacian
+ * for velocity, Gaussian R_h for the interface), inversion2d.f90:6578-7167. */
+int orc_lsqr_smooth(void* h, int smooth_type, int ndata, int nparm, const int* gindx,
+                    const double* gval, const int* row_ptr, const double* residual,
+                    const double* gtg_diag, const double* dm_sum, const double* mvscale,
+                    double corr_x, double corr_z, double corr_x_iface, double eps_min,
+                    double wdv, double wdv_iface, double w_smooth, double w_smooth_iface,
+                    int max_iter, double* dm, int* iters, double* rnorm, double* test2);
 /* Gaussian smoothing matrices of build_gauss_smooth_matrix (which 0: R_h,
  * 1: R_v) and build_iface_gauss_smooth_matrix (which 2), inversion2d.f90:
  * 1252-1616, as 1-based CSR over the model's parameters; returns nnz. */

@@ -71,6 +71,12 @@ def lib():
                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.orc_spmv.argtypes = [C.c_int, C.c_int, _ip, _dp, _ip, C.c_int, _dp, _dp]
     L.orc_laplacian.argtypes = [V, C.c_int, _dp, _dp]
+    L.orc_lsqr_smooth.argtypes = [V, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p,
+                                  C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]
     L.orc_gauss_smooth.restype = C.c_int
     L.orc_gauss_smooth.argtypes = [V, C.c_double, C.c_double, C.c_double, _dp, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
@@ -201,6 +207,26 @@ class Oracle:
                                rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
                                val.ctypes.data_as(C.c_void_p), n)
         return rp, col[:n], val[:n]
+
+    def lsqr_smooth(self, smooth_type, ndata, nparm, gindx, gval, row_ptr, residual, gtg, dm_sum,
+                    mvscale, corr_x, corr_z, corr_x_iface, eps_min, wdv, wdv_iface, w_smooth,
+                    w_smooth_iface, max_iter):
+        """run_lsqr for smooth_type 1, 2 or 3; returns (dm, iters, rnorm, test2)."""
+        keep = []
+
+        def p(a, t):
+            a = np.ascontiguousarray(a, dtype=t)
+            keep.append(a)
+            return a.ctypes.data_as(C.c_void_p)
+        dm = np.zeros(nparm)
+        it, rn, t2 = C.c_int(), C.c_double(), C.c_double()
+        lib().orc_lsqr_smooth(self.h, smooth_type, ndata, nparm, p(gindx, np.int32),
+                              p(gval, np.float64), p(row_ptr, np.int32), p(residual, np.float64),
+                              p(gtg, np.float64), p(dm_sum, np.float64), p(mvscale, np.float64),
+                              corr_x, corr_z, corr_x_iface, eps_min, wdv, wdv_iface, w_smooth,
+                              w_smooth_iface, max_iter, dm.ctypes.data_as(C.c_void_p),
+                              C.byref(it), C.byref(rn), C.byref(t2))
+        return dm, it.value, rn.value, t2.value
 
     def laplacian(self, nparm, v):
         out = np.zeros(nparm)

@@ -261,6 +261,32 @@ void orc_laplacian(void* h, int nparm, const double* vin, double* vout) {
   orc::laplacian(G, nparm, vin, vout);
 }
 
+// run_lsqr for smooth_type 1, 2 or 3 (inversion2d.f90:6578-7167); the
+// Gaussian matrices are built here from corr_x / corr_z / corr_x_iface and
+// mvscale as lsqr_inversion2d builds them.
+int orc_lsqr_smooth(void* h, int smooth_type, int ndata, int nparm, const int* gindx,
+                    const double* gval, const int* row_ptr, const double* residual,
+                    const double* gtg_diag, const double* dm_sum, const double* mvscale,
+                    double corr_x, double corr_z, double corr_x_iface, double eps_min,
+                    double wdv, double wdv_iface, double w_smooth, double w_smooth_iface,
+                    int max_iter, double* dm, int* iters, double* rnorm, double* test2) {
+  const orc::Model& m = H(h)->m;
+  orc::LsqrGeom G;
+  G.nx = m.grid.nx; G.nz = m.grid.nz; G.inv_idx = m.inv_idx.data();
+  if (m.iface_inv > 0) { G.iface_start = m.iface_start; G.iface_nx = m.isec[m.iface_inv].nnode; }
+  orc::LsqrInput in;
+  in.ndata = ndata; in.nparm = nparm; in.n_vel_parms = m.n_vel_parms; in.max_iter = max_iter;
+  in.gindx = gindx; in.gval = gval; in.row_ptr = row_ptr; in.residual = residual;
+  in.gtg_diag = gtg_diag; in.dm_sum = dm_sum; in.eps_min = eps_min; in.wdv = wdv;
+  in.wdv_iface = wdv_iface; in.w_smooth = w_smooth; in.w_smooth_iface = w_smooth_iface;
+  orc::Csr rh, rv, ri;
+  if (smooth_type == 2) orc::gauss_smooth_matrices(m, nparm, corr_x, corr_z, mvscale, rh, rv);
+  if (smooth_type >= 2) orc::iface_gauss_smooth_matrix(m, nparm, corr_x_iface, mvscale, ri);
+  const orc::LsqrResult r = orc::run_lsqr_general(G, in, smooth_type, &rh, &rv, &ri, dm);
+  *iters = r.iters; *rnorm = r.rnorm; *test2 = r.test2;
+  return 0;
+}
+
 // Gaussian smoothing matrices: which 0 = R_h, 1 = R_v (velocity parameters),
 // 2 = interface R_h.  Writes the 1-based CSR (rp[nparm+1], col/val up to cap)
 // and returns nnz.

@@ -32,4 +32,12 @@ void sparse_ATx(int ndata, int nparm, const int* gindx, const double* gval, cons
 void laplacian(const LsqrGeom& G, int nparm, const double* vin, double* vout);
 LsqrResult run_lsqr_laplacian(const LsqrGeom& G, const LsqrInput& in, double* dm);
 
+struct Csr;
+// run_lsqr for every smooth_type: 1 = [G; w_s L; w_d I], 2 = [G; w_s R_h;
+// w_s R_v; w_d I] with the interface Gaussian ri in the R_h block's interface
+// rows, 3 = [G; w_s L (velocity) + w_si ri (interface); w_d I].  rh / rv / ri
+// are the 1-based CSRs of the Gaussian matrices (ri may be empty: not built).
+LsqrResult run_lsqr_general(const LsqrGeom& G, const LsqrInput& in, int smooth_type,
+                            const Csr* rh, const Csr* rv, const Csr* ri, double* dm);
+
 }  // namespace orc
