@@ -118,13 +118,19 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
   d_rowptr_.alloc((np + 1) * sizeof(int));
   if (!d_tcalc_.p || !d_valid_.p || !d_cnt_.p || !d_off_.p || !d_rowptr_.p)
     return "device allocation failed (picks)";
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, stream_);
+  // the timing events are released on every return
+  struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Events() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~Events() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } ev;
+  cudaEventRecord(ev.a, stream_);
   rows_ = 0;
   nnz_ = 0;
-  npick_ = npick;
+  npick_ = -1;   // no rows to hand out unless this trace completes
   if (npick > 0) {
     const TrModel* M = d_trmodel_.as<TrModel>();
     unsigned* cnt = d_cnt_.as<unsigned>();
@@ -224,13 +230,12 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
     TCK(cudaMemcpyAsync(t_calc, d_tcalc_.p, (size_t)npick * 8, cudaMemcpyDeviceToHost, stream_));
     TCK(cudaMemcpyAsync(valid, d_valid_.p, (size_t)npick * 4, cudaMemcpyDeviceToHost, stream_));
   }
-  cudaEventRecord(e1, stream_);
+  cudaEventRecord(ev.b, stream_);
   TCK(cudaStreamSynchronize(stream_));
   float ms = 0.0f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaEventElapsedTime(&ms, ev.a, ev.b);
   trace_ms_ = ms;
+  npick_ = npick;
   if (nnz) *nnz = nnz_;
   return std::string();
 }
