@@ -35,6 +35,33 @@ def fields_of(mask: int) -> list[int]:
     return sorted(out)
 
 
+def select_data(phase, obs, t_calc, valid, row_ptr, gindx, gval, mvscale, *, crit_chi,
+                wt_psed=1.0, wt_pmp=1.0, wt_pgss=1.0):
+    """read_frechet_data2d's selection with lsqr_inversion2d's weighting
+    (fmt2d_select_data) over a batch of traced picks and their 1-based CSR
+    rows.  Returns (row_ptr, gindx, gval, residual, data_wt, pick_of_row) of
+    the kept picks, ready for Fmt2d.set_frechet / Fmt2d.lsqr."""
+    L = N.lib()
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    phase, valid, row_ptr, gindx = i32(phase), i32(valid), i32(row_ptr), i32(gindx)
+    obs, t_calc, gval, mvscale = f64(obs), f64(t_calc), f64(gval), f64(mvscale)
+    n = phase.size
+    nnz = max(gindx.size, 1)
+    rp, gi, gv = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    res, wt, pk = np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1), np.int32)
+    nd = C.c_int()
+    rc = L.fmt2d_select_data(n, N.ptr(phase), N.ptr(obs), N.ptr(t_calc), N.ptr(valid),
+                             N.ptr(row_ptr), N.ptr(gindx), N.ptr(gval), mvscale.size,
+                             N.ptr(mvscale), float(crit_chi), float(wt_psed), float(wt_pmp),
+                             float(wt_pgss), C.byref(nd), N.ptr(rp), N.ptr(gi), N.ptr(gv),
+                             N.ptr(res), N.ptr(wt), N.ptr(pk))
+    if rc != 0:
+        raise N.Fmt2dError(f"fmt2d_select_data failed ({rc}): bad arguments")
+    k, kk = nd.value, int(rp[nd.value]) - 1
+    return rp[:k + 1], gi[:kk], gv[:kk], res[:k], wt[:k], pk[:k]
+
+
 class Fmt2d:
     """One context (device buffers + stream).  device=-1 gives a host-only
     context for the model tables."""

@@ -154,6 +154,28 @@ int fmt2d_gauss_smooth(fmt2d_ctx* ctx, int which, double corr_x, double corr_z,
   return FMT2D_OK;
 }
 
+int fmt2d_select_data(int npick, const int* phase, const double* obs, const double* t_calc,
+                      const int* valid, const int* row_ptr, const int* gindx, const double* gval,
+                      int nparm, const double* mvscale, double crit_chi, double wt_psed,
+                      double wt_pmp, double wt_pgss, int* ndata, int* row_ptr_out,
+                      int* gindx_out, double* gval_out, double* residual, double* data_wt,
+                      int* pick_of_row) {
+  if (npick < 0 || nparm <= 0 || !ndata || !row_ptr_out) return FMT2D_ERR_ARG;
+  if (npick > 0 && (!phase || !obs || !t_calc || !valid || !row_ptr || !mvscale || !residual ||
+                    !data_wt || !pick_of_row))
+    return FMT2D_ERR_ARG;
+  if (npick > 0 && row_ptr[npick] > row_ptr[0] && (!gindx || !gval || !gindx_out || !gval_out))
+    return FMT2D_ERR_ARG;
+  if (npick > 0 && row_ptr[0] != 1) return FMT2D_ERR_ARG;
+  for (int p = 0; p < npick; ++p)
+    if (row_ptr[p + 1] < row_ptr[p]) return FMT2D_ERR_ARG;
+  const double wt[3] = {wt_psed, wt_pmp, wt_pgss};
+  *ndata = fmt2d::select_data(npick, phase, obs, t_calc, valid, row_ptr, gindx, gval, nparm,
+                              mvscale, crit_chi, wt, row_ptr_out, gindx_out, gval_out, residual,
+                              data_wt, pick_of_row);
+  return FMT2D_OK;
+}
+
 int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* nvp, int* npar) {
   if (!ctx) return FMT2D_ERR_ARG;
   if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");

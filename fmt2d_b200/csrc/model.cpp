@@ -406,4 +406,33 @@ std::string gauss_smooth_csr(const Model& m, int which, double corr_x, double co
   return std::string();
 }
 
+int select_data(int npick, const int* phase, const double* obs, const double* t_calc,
+                const int* valid, const int* row_ptr, const int* gindx, const double* gval,
+                int nparm, const double* mvscale, double crit_chi, const double* phase_wt,
+                int* row_ptr_out, int* gindx_out, double* gval_out, double* residual,
+                double* data_wt, int* pick_of_row) {
+  int nd = 0, kk = 0;
+  row_ptr_out[0] = 1;
+  for (int p = 0; p < npick; ++p) {
+    if (!valid[p] || obs[p] < 0.0) continue;
+    const double res = obs[p] - t_calc[p];
+    if (std::fabs(res) > crit_chi) continue;
+    const int ph = phase[p];
+    const double wt = (ph == 2 || ph == 3) ? 1.0 * phase_wt[ph - 2]
+                      : (ph == 4 || ph == 5) ? 1.0 * phase_wt[2] : 1.0;
+    for (int k = row_ptr[p] - 1; k < row_ptr[p + 1] - 1; ++k) {
+      const int j = gindx[k];
+      gindx_out[kk] = j;
+      gval_out[kk] = (j >= 1 && j <= nparm) ? gval[k] * mvscale[j - 1] * wt : gval[k];
+      ++kk;
+    }
+    residual[nd] = res * wt;
+    data_wt[nd] = wt;
+    pick_of_row[nd] = p;
+    ++nd;
+    row_ptr_out[nd] = kk + 1;
+  }
+  return nd;
+}
+
 }  // namespace fmt2d

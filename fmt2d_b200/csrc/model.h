@@ -101,6 +101,15 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
 // parameters (build_gauss_smooth_matrix, src/inversion2d.f90:1252-1402),
 // 2 = R_h over the inverted interface (build_iface_gauss_smooth_matrix,
 // :1524-1616).  Returns an error message or "".
+// read_frechet_data2d's selection with lsqr_inversion2d's weighting
+// (src/inversion2d.f90:3965-4052, :334-379); see fmt2d_select_data.
+// phase_wt = {PsedP, PmP, Pg_ss and Pg_ss2}.  Returns ndata.
+int select_data(int npick, const int* phase, const double* obs, const double* t_calc,
+                const int* valid, const int* row_ptr, const int* gindx, const double* gval,
+                int nparm, const double* mvscale, double crit_chi, const double* phase_wt,
+                int* row_ptr_out, int* gindx_out, double* gval_out, double* residual,
+                double* data_wt, int* pick_of_row);
+
 std::string gauss_smooth_csr(const Model& m, int which, double corr_x, double corr_z,
                              double corr_x_iface, const double* mvscale, std::vector<int>& rp,
                              std::vector<int>& col, std::vector<double>& val);

@@ -95,6 +95,25 @@ FMT2D_API int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, doubl
  * fastest, 1-based ids, 0 inactive; returns counts. */
 FMT2D_API int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* n_vel_parms, int* n_inv_parms);
 
+/* The data of one LSQR solve from a batch of traced picks: the selection of
+ * read_frechet_data2d (src/inversion2d.f90:3965-4052) with the weighting of
+ * lsqr_inversion2d (:334-379).  Keeps, in pick order, the picks that are
+ * valid, have obs >= 0 and |obs - t_calc| <= crit_chi; data_wt is wt_psed for
+ * phase 2, wt_pmp for 3, wt_pgss for 4 and 5, else 1; residual = (obs -
+ * t_calc) * data_wt; the kept rows' values become gval * mvscale[j-1] *
+ * data_wt (columns 1..nparm; mvscale[nparm]).  Input rows: 1-based CSR over
+ * all npick picks, as fmt2d_frechet_rows returns them.  Outputs (sized for
+ * every pick kept): *ndata, row_ptr_out[ndata+1] (1-based), gindx_out and
+ * gval_out[nnz], residual, data_wt and pick_of_row (0-based) [ndata].  Host
+ * only, no context: it replaces Fortran array work, not a device routine. */
+FMT2D_API int fmt2d_select_data(int npick, const int* phase, const double* obs,
+                                const double* t_calc, const int* valid, const int* row_ptr,
+                                const int* gindx, const double* gval, int nparm,
+                                const double* mvscale, double crit_chi, double wt_psed,
+                                double wt_pmp, double wt_pgss, int* ndata, int* row_ptr_out,
+                                int* gindx_out, double* gval_out, double* residual,
+                                double* data_wt, int* pick_of_row);
+
 /* Gaussian smoothing matrix of run_lsqr's smooth_type 2/3 layouts, built on
  * the host (works on a host-only context): which 0 = R_h and 1 = R_v over the
  * velocity parameters (build_gauss_smooth_matrix, src/inversion2d.f90:
