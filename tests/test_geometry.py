@@ -16,7 +16,7 @@ def native():
     return Fmt2d
 
 
-@pytest.mark.parametrize("which", ["small", 0, 1])
+@pytest.mark.parametrize("which", ["small", 0, 1, 4])   # 4: the largest, 4001x601
 def test_region_and_parameter_numbering(oracle_lib, native, which):
     m = synth.small_model() if which == "small" else synth.config(which)
     o = oracle_lib.Oracle(m)
