@@ -67,6 +67,11 @@ def lib():
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
     L.fmt2d_set_schedule.argtypes = [V, C.c_int, C.c_double, C.c_int]
+    L.fmt2d_projection.argtypes = [V, C.c_int, C.c_int, C.c_int] + [P(C.c_int)] * 4 + \
+        [C.c_void_p] * 4 + [P(C.c_longlong)]
+    L.fmt2d_project_rows.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, P(C.c_longlong)]
     # npick, 7 input arrays, nparm, mvscale, crit_chi and 3 weights, 7 outputs
     L.fmt2d_select_data.argtypes = [C.c_int] + [C.c_void_p] * 7 + [C.c_int, C.c_void_p] + \
         [C.c_double] * 4 + [C.c_void_p] * 7

@@ -62,6 +62,25 @@ def select_data(phase, obs, t_calc, valid, row_ptr, gindx, gval, mvscale, *, cri
     return rp[:k + 1], gi[:kk], gv[:kk], res[:k], wt[:k], pk[:k]
 
 
+def project_rows(row_ptr, gindx, gval, nfine, p_row_ptr, p_col, p_val):
+    """Rows of G P (fmt2d_project_rows): 1-based CSR (row_ptr, gindx, gval)
+    over the fine parameters mapped onto a coarse grid's parameters."""
+    L = N.lib()
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    rp, gi, gv = i32(row_ptr), i32(gindx), f64(gval)
+    prp, pc, pv = i32(p_row_ptr), i32(p_col), f64(p_val)
+    nd = rp.size - 1
+    nnz = C.c_longlong()
+    args = (nd, N.ptr(rp), N.ptr(gi), N.ptr(gv), int(nfine), N.ptr(prp), N.ptr(pc), N.ptr(pv))
+    if L.fmt2d_project_rows(*args, None, None, None, C.byref(nnz)) != 0:
+        raise N.Fmt2dError("fmt2d_project_rows: bad arguments")
+    orp = np.zeros(nd + 1, np.int32)
+    ogi, ogv = np.zeros(max(nnz.value, 1), np.int32), np.zeros(max(nnz.value, 1))
+    L.fmt2d_project_rows(*args, N.ptr(orp), N.ptr(ogi), N.ptr(ogv), C.byref(nnz))
+    return orp, ogi[:nnz.value], ogv[:nnz.value]
+
+
 class Fmt2d:
     """One context (device buffers + stream).  device=-1 gives a host-only
     context for the model tables."""
@@ -136,6 +155,25 @@ class Fmt2d:
         self._check(self.L.fmt2d_inv_index(self.h, N.ptr(out), C.byref(nvp), C.byref(npar)),
                     "fmt2d_inv_index")
         return out.reshape(self.nz, self.nx), nvp.value, npar.value
+
+    def projection(self, kx: int, kz: int, ki: int) -> dict:
+        """Coarse inversion grid every kx columns / kz rows (interface every
+        ki nodes) and its projection P onto the model's parameters
+        (fmt2d_projection).  Returns dict(P=(row_ptr, col, val), nvp, npar,
+        coarse_idx (nzc, nxc))."""
+        nxc, nzc, nvp, npar, nnz = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_longlong()
+        sizes = (C.byref(nxc), C.byref(nzc), C.byref(nvp), C.byref(npar))
+        self._check(self.L.fmt2d_projection(self.h, kx, kz, ki, *sizes, None, None, None, None,
+                                            C.byref(nnz)), "fmt2d_projection")
+        nfine = self.inv_index()[2]
+        cidx = np.zeros(nxc.value * nzc.value, np.int32)
+        rp = np.zeros(nfine + 1, np.int32)
+        col, val = np.zeros(max(nnz.value, 1), np.int32), np.zeros(max(nnz.value, 1))
+        self._check(self.L.fmt2d_projection(self.h, kx, kz, ki, *sizes, N.ptr(cidx), N.ptr(rp),
+                                            N.ptr(col), N.ptr(val), C.byref(nnz)),
+                    "fmt2d_projection")
+        return dict(P=(rp, col[:nnz.value], val[:nnz.value]), nvp=nvp.value, npar=npar.value,
+                    coarse_idx=cidx.reshape(nzc.value, nxc.value))
 
     def gauss_smooth(self, which: int, mvscale, corr_x=0.0, corr_z=0.0, corr_x_iface=0.0):
         """1-based CSR (row_ptr, col, val) of the Gaussian smoothing matrix R_h

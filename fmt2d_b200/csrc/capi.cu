@@ -176,6 +176,45 @@ int fmt2d_select_data(int npick, const int* phase, const double* obs, const doub
   return FMT2D_OK;
 }
 
+int fmt2d_projection(fmt2d_ctx* ctx, int kx, int kz, int ki, int* nxc, int* nzc, int* nvp_c,
+                     int* npar_c, int* coarse_idx, int* p_row_ptr, int* p_col, double* p_val,
+                     long long* p_nnz) {
+  if (!ctx || !nxc || !nzc || !nvp_c || !npar_c || !p_nnz) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  std::vector<int> cidx, rp, col;
+  std::vector<double> val;
+  const std::string e = fmt2d::projection(ctx->model, kx, kz, ki, cidx, *nxc, *nzc, *nvp_c,
+                                          *npar_c, rp, col, val);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  *p_nnz = (long long)col.size();
+  if (coarse_idx) std::copy(cidx.begin(), cidx.end(), coarse_idx);
+  if (p_row_ptr) std::copy(rp.begin(), rp.end(), p_row_ptr);
+  if (p_col) std::copy(col.begin(), col.end(), p_col);
+  if (p_val) std::copy(val.begin(), val.end(), p_val);
+  return FMT2D_OK;
+}
+
+int fmt2d_project_rows(int ndata, const int* row_ptr, const int* gindx, const double* gval,
+                       int nfine, const int* p_row_ptr, const int* p_col, const double* p_val,
+                       int* row_ptr_out, int* gindx_out, double* gval_out, long long* nnz) {
+  if (ndata < 0 || nfine <= 0 || !row_ptr || !p_row_ptr || !nnz) return FMT2D_ERR_ARG;
+  if (row_ptr[0] != 1 || p_row_ptr[0] != 1) return FMT2D_ERR_ARG;
+  for (int i = 0; i < ndata; ++i)
+    if (row_ptr[i + 1] < row_ptr[i]) return FMT2D_ERR_ARG;
+  for (int f = 0; f < nfine; ++f)
+    if (p_row_ptr[f + 1] < p_row_ptr[f]) return FMT2D_ERR_ARG;
+  if (row_ptr[ndata] > 1 && (!gindx || !gval)) return FMT2D_ERR_ARG;
+  if (p_row_ptr[nfine] > 1 && (!p_col || !p_val)) return FMT2D_ERR_ARG;
+  std::vector<int> rp, col;
+  std::vector<double> val;
+  fmt2d::project_rows(ndata, row_ptr, gindx, gval, nfine, p_row_ptr, p_col, p_val, rp, col, val);
+  *nnz = (long long)col.size();
+  if (row_ptr_out) std::copy(rp.begin(), rp.end(), row_ptr_out);
+  if (gindx_out) std::copy(col.begin(), col.end(), gindx_out);
+  if (gval_out) std::copy(val.begin(), val.end(), gval_out);
+  return FMT2D_OK;
+}
+
 int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* nvp, int* npar) {
   if (!ctx) return FMT2D_ERR_ARG;
   if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");

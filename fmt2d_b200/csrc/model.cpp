@@ -406,6 +406,98 @@ std::string gauss_smooth_csr(const Model& m, int which, double corr_x, double co
   return std::string();
 }
 
+std::string projection(const Model& m, int kx, int kz, int ki, std::vector<int>& coarse_idx,
+                       int& nxc, int& nzc, int& nvp_c, int& npar_c, std::vector<int>& rp,
+                       std::vector<int>& col, std::vector<double>& val) {
+  if (kx < 1 || kz < 1 || ki < 1) return "refinement ratios must be >= 1";
+  nxc = (m.nx - 1 + kx - 1) / kx + 1;
+  nzc = (m.nz - 1 + kz - 1) / kz + 1;
+  // corners and weights of each fine velocity parameter: fine node (ix, iz)
+  // lies in coarse cell (ix / kx, iz / kz) at fractions (ix % kx) / kx,
+  // (iz % kz) / kz, exact for integer ratios (ratio 1 gives weight 1)
+  struct W { int c[4]; double w[4]; };
+  std::vector<W> fw(m.n_vel_parms + 1);
+  std::vector<uint8_t> used((size_t)nxc * nzc, 0);
+  for (int iz = 0; iz < m.nz; ++iz)
+    for (int ix = 0; ix < m.nx; ++ix) {
+      const int f = m.inv_idx[m.g(ix, iz)];
+      if (f <= 0) continue;
+      const int i = ix / kx, j = iz / kz;
+      const double a = (double)(ix % kx) / kx, b = (double)(iz % kz) / kz;
+      W& w = fw[f];
+      const int ci[4] = {i, i + 1, i, i + 1}, cj[4] = {j, j, j + 1, j + 1};
+      const double ww[4] = {(1.0 - a) * (1.0 - b), a * (1.0 - b), (1.0 - a) * b, a * b};
+      for (int k = 0; k < 4; ++k) {
+        const bool in = ci[k] < nxc && cj[k] < nzc && ww[k] != 0.0;
+        w.c[k] = in ? cj[k] * nxc + ci[k] : -1;
+        w.w[k] = ww[k];
+        if (in) used[(size_t)w.c[k]] = 1;
+      }
+    }
+  // coarse velocity parameters: the touched coarse nodes, iz outer / ix inner
+  coarse_idx.assign((size_t)nxc * nzc, 0);
+  nvp_c = 0;
+  for (size_t c = 0; c < used.size(); ++c)
+    if (used[c]) coarse_idx[c] = ++nvp_c;
+  // coarse interface nodes every ki fine interface nodes
+  const int nic = m.iface_inv > 0 ? (m.nx - 1 + ki - 1) / ki + 1 : 0;
+  npar_c = nvp_c + nic;
+  rp.assign(m.n_inv_parms + 1, 1);
+  col.clear();
+  val.clear();
+  for (int f = 1; f <= m.n_inv_parms; ++f) {
+    if (f <= m.n_vel_parms) {
+      const W& w = fw[f];
+      for (int k = 0; k < 4; ++k)
+        if (w.c[k] >= 0) {
+          col.push_back(coarse_idx[(size_t)w.c[k]]);
+          val.push_back(w.w[k]);
+        }
+    } else {
+      const int ix = f - m.n_vel_parms - 1, i = ix / ki;
+      const double a = (double)(ix % ki) / ki;
+      col.push_back(nvp_c + i + 1);
+      val.push_back(1.0 - a);
+      if (a != 0.0 && i + 1 < nic) {
+        col.push_back(nvp_c + i + 2);
+        val.push_back(a);
+      }
+    }
+    rp[f] = (int)col.size() + 1;
+  }
+  return std::string();
+}
+
+void project_rows(int ndata, const int* row_ptr, const int* gindx, const double* gval,
+                  int nfine, const int* prp, const int* pcol, const double* pval,
+                  std::vector<int>& rp, std::vector<int>& col, std::vector<double>& val) {
+  rp.assign(ndata + 1, 1);
+  col.clear();
+  val.clear();
+  std::vector<std::pair<int, double>> acc;
+  for (int i = 0; i < ndata; ++i) {
+    acc.clear();
+    for (int k = row_ptr[i] - 1; k < row_ptr[i + 1] - 1; ++k) {
+      const int f = gindx[k];
+      if (f < 1 || f > nfine) continue;
+      for (int q = prp[f - 1] - 1; q < prp[f] - 1; ++q) acc.emplace_back(pcol[q], gval[k] * pval[q]);
+    }
+    // ascending coarse columns; equal columns summed in the order of the fine entries
+    std::stable_sort(acc.begin(), acc.end(),
+                     [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+                       return a.first < b.first;
+                     });
+    for (size_t q = 0; q < acc.size();) {
+      double s = 0.0;
+      const int c = acc[q].first;
+      for (; q < acc.size() && acc[q].first == c; ++q) s = s + acc[q].second;
+      col.push_back(c);
+      val.push_back(s);
+    }
+    rp[i + 1] = (int)col.size() + 1;
+  }
+}
+
 int select_data(int npick, const int* phase, const double* obs, const double* t_calc,
                 const int* valid, const int* row_ptr, const int* gindx, const double* gval,
                 int nparm, const double* mvscale, double crit_chi, const double* phase_wt,

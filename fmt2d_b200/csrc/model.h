@@ -101,6 +101,23 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
 // parameters (build_gauss_smooth_matrix, src/inversion2d.f90:1252-1402),
 // 2 = R_h over the inverted interface (build_iface_gauss_smooth_matrix,
 // :1524-1616).  Returns an error message or "".
+// Projection P from a coarse inversion grid onto the model's parameters
+// (fine velocity parameters = bilinear interpolation of coarse nodes every kx
+// columns and kz rows; fine interface parameters = linear interpolation of
+// coarse interface nodes every ki nodes).  P is a 1-based CSR with one row per
+// fine parameter; coarse velocity parameters are the coarse nodes some fine
+// parameter uses, numbered iz outer / ix inner (coarse_idx over nzc x nxc,
+// 0 unused), coarse interface parameters follow.  kx = kz = ki = 1 gives
+// P = I.
+std::string projection(const Model& m, int kx, int kz, int ki, std::vector<int>& coarse_idx,
+                       int& nxc, int& nzc, int& nvp_c, int& npar_c, std::vector<int>& rp,
+                       std::vector<int>& col, std::vector<double>& val);
+// Rows of G P: each row's fine entries mapped through P, coarse columns
+// ascending (1-based CSR in and out; columns outside 1..nfine ignored).
+void project_rows(int ndata, const int* row_ptr, const int* gindx, const double* gval,
+                  int nfine, const int* prp, const int* pcol, const double* pval,
+                  std::vector<int>& rp, std::vector<int>& col, std::vector<double>& val);
+
 // read_frechet_data2d's selection with lsqr_inversion2d's weighting
 // (src/inversion2d.f90:3965-4052, :334-379); see fmt2d_select_data.
 // phase_wt = {PsedP, PmP, Pg_ss and Pg_ss2}.  Returns ndata.

@@ -95,6 +95,30 @@ FMT2D_API int fmt2d_region_geometry(fmt2d_ctx* ctx, int region, double* x, doubl
  * fastest, 1-based ids, 0 inactive; returns counts. */
 FMT2D_API int fmt2d_inv_index(fmt2d_ctx* ctx, int* inv_idx, int* n_vel_parms, int* n_inv_parms);
 
+/* A coarse inversion grid over the model's parameters (no reference
+ * counterpart: the reference inverts on the propagation grid itself, which
+ * is kx = kz = ki = 1 and gives P = I).  Coarse velocity nodes every kx grid
+ * columns and kz grid rows, coarse interface nodes every ki interface nodes;
+ * each fine velocity parameter is the bilinear interpolation of its coarse
+ * cell's corners, each fine interface parameter the linear interpolation of
+ * its two coarse interface nodes.  Returns the coarse grid size (*nxc, *nzc),
+ * *nvp_c coarse velocity parameters (the coarse nodes some fine parameter
+ * uses, numbered iz outer / ix inner in coarse_idx[nzc*nxc], 0 unused),
+ * *npar_c with the coarse interface parameters after them, and P as 1-based
+ * CSR: p_row_ptr[n_inv_parms + 1], p_col / p_val[*p_nnz].  Any array may be
+ * NULL (sizes first).  Host-side: works on a host-only context. */
+FMT2D_API int fmt2d_projection(fmt2d_ctx* ctx, int kx, int kz, int ki, int* nxc, int* nzc,
+                               int* nvp_c, int* npar_c, int* coarse_idx, int* p_row_ptr,
+                               int* p_col, double* p_val, long long* p_nnz);
+/* Rows of G P for a 1-based CSR G over nfine fine parameters and P from
+ * fmt2d_projection: coarse columns ascending, equal columns summed in the
+ * order of the fine entries.  Outputs may be NULL to get *nnz first.  Host
+ * only, no context. */
+FMT2D_API int fmt2d_project_rows(int ndata, const int* row_ptr, const int* gindx,
+                                 const double* gval, int nfine, const int* p_row_ptr,
+                                 const int* p_col, const double* p_val, int* row_ptr_out,
+                                 int* gindx_out, double* gval_out, long long* nnz);
+
 /* The data of one LSQR solve from a batch of traced picks: the selection of
  * read_frechet_data2d (src/inversion2d.f90:3965-4052) with the weighting of
  * lsqr_inversion2d (:334-379).  Keeps, in pick order, the picks that are
