@@ -75,6 +75,15 @@ int orc_lsqr_smooth(void* h, int smooth_type, int ndata, int nparm, const int* g
                     double corr_x, double corr_z, double corr_x_iface, double eps_min,
                     double wdv, double wdv_iface, double w_smooth, double w_smooth_iface,
                     int max_iter, double* dm, int* iters, double* rnorm, double* test2);
+/* run_lsqr (smooth_type 1) with the Laplacian on an explicit parameter grid
+ * (inv_idx over gnz x gnx, ix fastest; iface_nx interface parameters after
+ * the n_vel_parms velocity parameters). */
+int orc_lsqr_geom(int gnx, int gnz, const int* inv_idx, int n_vel_parms, int iface_nx,
+                  int ndata, int nparm, const int* gindx, const double* gval,
+                  const int* row_ptr, const double* residual, const double* gtg_diag,
+                  const double* dm_sum, double eps_min, double wdv, double wdv_iface,
+                  double w_smooth, double w_smooth_iface, int max_iter, double* dm, int* iters,
+                  double* rnorm, double* test2);
 /* Gaussian smoothing matrices of build_gauss_smooth_matrix (which 0: R_h,
  * 1: R_v) and build_iface_gauss_smooth_matrix (which 2), inversion2d.f90:
  * 1252-1616, as 1-based CSR over the model's parameters; returns nnz. */

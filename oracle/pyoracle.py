@@ -77,6 +77,9 @@ def lib():
                                   C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p,
                                   C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]
+    L.orc_lsqr_geom.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                C.c_int] + [C.c_void_p] * 6 + [C.c_double] * 5 + \
+        [C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.orc_gauss_smooth.restype = C.c_int
     L.orc_gauss_smooth.argtypes = [V, C.c_double, C.c_double, C.c_double, _dp, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
@@ -232,6 +235,28 @@ class Oracle:
         out = np.zeros(nparm)
         lib().orc_laplacian(self.h, nparm, np.ascontiguousarray(v, dtype=np.float64), out)
         return out
+
+
+def lsqr_geom(inv_idx, n_vel_parms, iface_nx, ndata, nparm, gindx, gval, row_ptr, residual, gtg,
+              dm_sum, eps_min, wdv, wdv_iface, w_smooth, w_smooth_iface, max_iter):
+    """run_lsqr (smooth_type 1) with the Laplacian on the parameter grid
+    inv_idx (nz, nx); returns (dm, iters, rnorm, test2)."""
+    keep = []
+
+    def p(a, t):
+        a = np.ascontiguousarray(a, dtype=t)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+    inv = np.ascontiguousarray(inv_idx, dtype=np.int32)
+    dm = np.zeros(nparm)
+    it, rn, t2 = C.c_int(), C.c_double(), C.c_double()
+    lib().orc_lsqr_geom(inv.shape[1], inv.shape[0], p(inv, np.int32), n_vel_parms, iface_nx,
+                        ndata, nparm, p(gindx, np.int32), p(gval, np.float64),
+                        p(row_ptr, np.int32), p(residual, np.float64), p(gtg, np.float64),
+                        p(dm_sum, np.float64), eps_min, wdv, wdv_iface, w_smooth, w_smooth_iface,
+                        max_iter, dm.ctypes.data_as(C.c_void_p), C.byref(it), C.byref(rn),
+                        C.byref(t2))
+    return dm, it.value, rn.value, t2.value
 
 
 def spmv(ndata, nparm, gindx, gval, row_ptr, x, transpose=False):

@@ -287,6 +287,29 @@ int orc_lsqr_smooth(void* h, int smooth_type, int ndata, int nparm, const int* g
   return 0;
 }
 
+// run_lsqr (smooth_type 1) with the Laplacian on an explicit parameter grid:
+// inv_idx over nz x nx (ix fastest, 0 unused) numbers n_vel_parms velocity
+// parameters, and iface_nx interface parameters follow them (a coarse
+// inversion grid of the projection, or the propagation grid itself).
+int orc_lsqr_geom(int gnx, int gnz, const int* inv_idx, int n_vel_parms, int iface_nx,
+                  int ndata, int nparm, const int* gindx, const double* gval,
+                  const int* row_ptr, const double* residual, const double* gtg_diag,
+                  const double* dm_sum, double eps_min, double wdv, double wdv_iface,
+                  double w_smooth, double w_smooth_iface, int max_iter, double* dm, int* iters,
+                  double* rnorm, double* test2) {
+  orc::LsqrGeom G;
+  G.nx = gnx; G.nz = gnz; G.inv_idx = inv_idx;
+  if (iface_nx > 0) { G.iface_start = n_vel_parms; G.iface_nx = iface_nx; }
+  orc::LsqrInput in;
+  in.ndata = ndata; in.nparm = nparm; in.n_vel_parms = n_vel_parms; in.max_iter = max_iter;
+  in.gindx = gindx; in.gval = gval; in.row_ptr = row_ptr; in.residual = residual;
+  in.gtg_diag = gtg_diag; in.dm_sum = dm_sum; in.eps_min = eps_min; in.wdv = wdv;
+  in.wdv_iface = wdv_iface; in.w_smooth = w_smooth; in.w_smooth_iface = w_smooth_iface;
+  const orc::LsqrResult r = orc::run_lsqr_laplacian(G, in, dm);
+  *iters = r.iters; *rnorm = r.rnorm; *test2 = r.test2;
+  return 0;
+}
+
 // Gaussian smoothing matrices: which 0 = R_h, 1 = R_v (velocity parameters),
 // 2 = interface R_h.  Writes the 1-based CSR (rp[nparm+1], col/val up to cap)
 // and returns nnz.

@@ -102,3 +102,34 @@ def test_errors(small):
     bad[0] = 0
     with pytest.raises(N.Fmt2dError):
         project_rows(bad, gi, gv, npar, *g.projection(1, 1, 1)["P"])
+
+
+def test_lsqr_on_coarse_grid(small, oracle_lib):
+    """LSQR with the Laplacian on the coarse parameter grid (the oracle's
+    run_lsqr with an explicit geometry): at ratio 1 it is the model-grid solve
+    bit for bit; on a coarse grid it fits data made by a coarse model."""
+    from fmt2d_b200.api import project_rows
+    m, g, (nd, npar, rp, gi, gv) = small
+    o = oracle_lib.Oracle(m)
+    rng = np.random.default_rng(21)
+    r = rng.normal(0.0, 0.05, nd)
+    G = _csr(rp, gi, gv, npar)
+    gtg = np.asarray(G.multiply(G).sum(axis=0)).ravel()
+    eps_min = max(1e-6, 1e-4 * gtg.max())
+    inv, nvp, _ = g.inv_index()
+    a = o.lsqr(nd, npar, gi, gv, rp, r, gtg, np.zeros(npar), eps_min, 0.5, 0.5, 3.0, 3.0, 60)
+    b = oracle_lib.lsqr_geom(inv, nvp, npar - nvp, nd, npar, gi, gv, rp, r, gtg, np.zeros(npar),
+                             eps_min, 0.5, 0.5, 3.0, 3.0, 60)
+    assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+    pr = g.projection(4, 2, 4)
+    prp, pcol, pval = pr["P"]
+    npc, nvpc = pr["npar"], pr["nvp"]
+    crp, cgi, cgv = project_rows(rp, gi, gv, npar, prp, pcol, pval)
+    Gc = _csr(crp, cgi, cgv, npc)
+    x_true = np.concatenate([0.01 * rng.standard_normal(nvpc), 0.2 * rng.standard_normal(npc - nvpc)])
+    d = Gc @ x_true
+    gtgc = np.asarray(Gc.multiply(Gc).sum(axis=0)).ravel()
+    dm, it, rn, t2 = oracle_lib.lsqr_geom(pr["coarse_idx"], nvpc, npc - nvpc, nd, npc, cgi, cgv,
+                                          crp, d, gtgc, np.zeros(npc), 1e-12 * gtgc.max(), 0.0,
+                                          0.0, 0.0, 0.0, 400)
+    assert np.linalg.norm(Gc @ dm - d) < 0.05 * np.linalg.norm(d)
