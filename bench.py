@@ -81,19 +81,22 @@ def _cpu_worker(args):
 
 
 def cpu_fields_per_s(nsrc: int, procs: int, reps: int = 1):
-    """Fields/s of the CPU restatement over `nsrc` sources on `procs` processes."""
+    """Fields/s of the CPU restatement over `nsrc` sources on `procs` processes,
+    the processes' mean single-core rate and the wall times."""
     from fmt2d_b200.api import fields_of, phase_mask
     nf_src = len(fields_of(phase_mask(PHASES)))
     ctx = mp.get_context("spawn")
     chunks = [list(range(i, nsrc, procs)) for i in range(procs)]
     chunks = [c for c in chunks if c]
     with ctx.Pool(len(chunks), initializer=_cpu_init) as pool:
-        walls = []
+        walls, rates = [], []
         for _ in range(reps):
             t0 = time.perf_counter()
-            pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
+            secs = pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
             walls.append(time.perf_counter() - t0)
-    return nsrc * nf_src / float(np.median(walls)), len(chunks), walls
+            rates += [len(c) * nf_src / t for c, t in zip(chunks, secs) if t > 0]
+    one = float(np.mean(rates)) if rates else 0.0
+    return nsrc * nf_src / float(np.median(walls)), len(chunks), walls, one
 
 
 # ---------------------------------------------------------------- clocks
@@ -209,13 +212,14 @@ def run_reference(args, world, rank):
     ctx = mp.get_context("spawn")
     procs = min(cores, nsrc)
     chunks = [list(range(i, nsrc, procs)) for i in range(procs)]
-    walls = []
+    walls, rates = [], []
     with ctx.Pool(procs, initializer=_cpu_init) as pool:
         for step in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
+            secs = pool.map(_cpu_worker, [(c, PHASES) for c in chunks])
             if step >= args.warmup:
                 walls.append(time.perf_counter() - t0)
+                rates += [len(c) * nf_src / t for c, t in zip(chunks, secs) if t > 0]
     sec = float(np.sum(walls))
     value = nsrc * nf_src * len(walls) / sec
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "fields/s",
@@ -227,7 +231,10 @@ def run_reference(args, world, rank):
            "cpu_baseline": {"value": round(value, 3), "unit": "fields/s", "cores": procs,
                             "kind": "port",
                             "sample": f"{nsrc} of {nsrc_all} sources x Pg+PmP stages per step, "
-                                      f"FP64 heap fast marching, {procs} processes"},
+                                      f"FP64 heap fast marching, {procs} processes",
+                            "single_core": {"value": round(float(np.mean(rates)), 3)
+                                            if rates else None, "unit": "fields/s",
+                                            "sample": "mean rate of one process (one core)"}},
            "e2e": {"value": round(value, 3), "unit": "fields/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0},
            "gpu_launches": 0}
@@ -241,10 +248,12 @@ def run_ours(args, world, rank, local):
         cores = os.cpu_count() or 1
         nsrc = min(30, max(4, cores))
         procs = min(cores, nsrc)
-        v, used, walls = cpu_fields_per_s(nsrc, procs)
+        v, used, walls, one = cpu_fields_per_s(nsrc, procs)
         cpu = {"value": round(v, 3), "unit": "fields/s", "cores": used, "kind": "port",
                "sample": f"{nsrc} sources x Pg+PmP stages of the same model, FP64 heap fast "
-                         f"marching, {used} processes, {walls[0]:.1f} s wall"}
+                         f"marching, {used} processes, {walls[0]:.1f} s wall",
+               "single_core": {"value": round(one, 3), "unit": "fields/s",
+                               "sample": "mean rate of one process (one core) in that run"}}
     import torch
     from fmt2d_b200 import synth
     from fmt2d_b200.api import Fmt2d, fields_of, phase_mask, TF_REGION
@@ -312,6 +321,26 @@ def run_ours(args, world, rank, local):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world, dev)
     e2e_value = world * nf / e2e_s
 
+    # ---- the plain form, one source (its stage solves) per fmt2d_forward call,
+    # on a few sources: the denominator of "batched vs plain"; outside the
+    # timed region and never allowed to cost the main line
+    try:
+        k = int(min(3, src.size))
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for i in range(k):
+            g.forward(src[i:i + 1], PHASES)
+        p1.record(stream)
+        p1.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+        plain = {"value": round(k * len(fields_of(mask)) / (plain_ms / 1e3), 3),
+                 "unit": "fields/s", "sources_timed": k,
+                 "note": "one source per fmt2d_forward call, device-timed"}
+    except Exception as ex:  # the batched line is the result; report why this is absent
+        plain = {"unavailable": str(ex)[:200]}
+
     if rank != 0:
         return
     peak, peak_kind = measured_peak_hbm()
@@ -333,6 +362,7 @@ def run_ours(args, world, rank, local):
                         "frac": round(achieved / peak, 6) if achieved else None,
                         "peak_kind": peak_kind, "traffic": None,
                         "algorithmic_bytes_per_step": alg_bytes},
+           "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "cpu_baseline": cpu}
     print(json.dumps(out), flush=True)
