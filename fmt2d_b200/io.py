@@ -1,0 +1,141 @@
+"""The reference's input files (read_tomo2d.f90) for this library: readers
+(fmt2d_read_smesh / fmt2d_read_refl / fmt2d_read_geom, Fortran list-directed
+rules), writers of the same formats, and `model_from_files`, which turns a
+velocity mesh, the sediment-base and Moho files and a geometry file into the
+model descriptor and picks that `Fmt2d.upload` / `Fmt2d.forward` /
+`Fmt2d.trace` take."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .synth import SmeshModel
+
+
+def _err(rc: int, what: str):
+    if rc != 0:
+        buf = C.create_string_buffer(512)
+        N.lib().fmt2d_io_last_error(buf, 512)
+        raise N.Fmt2dError(f"{what} failed ({rc}): {buf.value.decode()}")
+
+
+def read_smesh(path: str) -> dict:
+    """read_smesh (read_tomo2d.f90:8-81): xpos, topo, zpos_rel and vel as
+    (nz, nx) (row iz at depth zpos_rel[iz] below the seafloor)."""
+    L = N.lib()
+    nx, nz, vw, va = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+    p = str(path).encode()
+    _err(L.fmt2d_read_smesh(p, C.byref(nx), C.byref(nz), C.byref(vw), C.byref(va), None, None,
+                            None, None), "fmt2d_read_smesh")
+    x, t, z = np.zeros(nx.value), np.zeros(nx.value), np.zeros(nz.value)
+    v = np.zeros(nx.value * nz.value)
+    _err(L.fmt2d_read_smesh(p, C.byref(nx), C.byref(nz), C.byref(vw), C.byref(va), N.ptr(x),
+                            N.ptr(t), N.ptr(z), N.ptr(v)), "fmt2d_read_smesh")
+    return dict(xpos=x, topo=t, zrel=z, vel=v.reshape(nz.value, nx.value), vwater=vw.value,
+                vair=va.value)
+
+
+def read_refl(path: str):
+    """read_refl (read_tomo2d.f90:83-139): the (x, z) nodes of an interface."""
+    L = N.lib()
+    n = C.c_int()
+    p = str(path).encode()
+    _err(L.fmt2d_read_refl(p, C.byref(n), None, None), "fmt2d_read_refl")
+    x, z = np.zeros(n.value), np.zeros(n.value)
+    _err(L.fmt2d_read_refl(p, C.byref(n), N.ptr(x), N.ptr(z)), "fmt2d_read_refl")
+    return x, z
+
+
+def read_geom(path: str) -> dict:
+    """read_geom (read_tomo2d.f90:141-248): OBS positions and, per receiver
+    (shot), its position, 1-based OBS id, phase, observed time and
+    uncertainty."""
+    L = N.lib()
+    no, nr = C.c_int(), C.c_int()
+    p = str(path).encode()
+    _err(L.fmt2d_read_geom(p, C.byref(no), C.byref(nr), *([None] * 8)), "fmt2d_read_geom")
+    ox, oz = np.zeros(no.value), np.zeros(no.value)
+    rx, rz, to, un = (np.zeros(nr.value) for _ in range(4))
+    oid, ph = np.zeros(nr.value, np.int32), np.zeros(nr.value, np.int32)
+    _err(L.fmt2d_read_geom(p, C.byref(no), C.byref(nr), N.ptr(ox), N.ptr(oz), N.ptr(rx),
+                           N.ptr(rz), N.ptr(oid), N.ptr(ph), N.ptr(to), N.ptr(un)),
+         "fmt2d_read_geom")
+    return dict(obs_x=ox, obs_z=oz, rec_x=rx, rec_z=rz, obs_id=oid, phase=ph, t_obs=to, unc=un)
+
+
+def write_smesh(path: str, xpos, topo, zrel, vel, vwater: float, vair: float = 0.33):
+    """A velocity mesh in read_smesh's format; vel is (nz, nx)."""
+    vel = np.asarray(vel, dtype=np.float64)
+    with open(path, "w") as f:
+        f.write(f"{len(xpos)} {len(zrel)} {float(vwater)!r} {float(vair)!r}\n")
+        for a in (xpos, topo, zrel):
+            f.write(" ".join(repr(float(v)) for v in a) + "\n")
+        for ix in range(vel.shape[1]):
+            f.write(" ".join(repr(float(v)) for v in vel[:, ix]) + "\n")
+
+
+def write_refl(path: str, x, z):
+    """An interface in read_refl's format."""
+    with open(path, "w") as f:
+        for a, b in zip(x, z):
+            f.write(f"{float(a)!r} {float(b)!r}\n")
+
+
+def write_geom(path: str, obs_x, obs_z, picks, t_obs=None, unc=None):
+    """Shot geometry and picks in read_geom's format; picks columns: source
+    index (0-based), phase, shot x, shot z (a negative t_obs marks a pick
+    without an observation)."""
+    picks = np.asarray(picks, dtype=np.float64).reshape(-1, 4)
+    t_obs = np.full(len(picks), -1.0) if t_obs is None else np.asarray(t_obs, dtype=np.float64)
+    unc = np.full(len(picks), 0.05) if unc is None else np.asarray(unc, dtype=np.float64)
+    with open(path, "w") as f:
+        f.write(f"{len(obs_x)}\n")
+        for s, (ox, oz) in enumerate(zip(obs_x, obs_z)):
+            k = np.where(picks[:, 0] == s)[0]
+            f.write(f"s {float(ox)!r} {float(oz)!r} {len(k)}\n")
+            for i in k:
+                f.write(f"r {float(picks[i, 2])!r} {float(picks[i, 3])!r} {int(picks[i, 1])} "
+                        f"{float(t_obs[i])!r} {float(unc[i])!r}\n")
+
+
+def iface_on_grid(x_nodes, z_nodes, xpos) -> np.ndarray:
+    """Depths of an interface at the grid's x: linear between its nodes,
+    clamped at its ends, with the node spacing x(2) - x(1) as
+    interpolate_iface_z_inv reads it (src/inversion2d.f90)."""
+    xn, zn = np.asarray(x_nodes, dtype=np.float64), np.asarray(z_nodes, dtype=np.float64)
+    out = np.empty(len(xpos))
+    if xn.size < 2:
+        out[:] = zn[0]
+        return out
+    dx = xn[1] - xn[0]
+    for k, px in enumerate(np.asarray(xpos, dtype=np.float64)):
+        i = int(np.floor((px - xn[0]) / dx)) + 1
+        if i < 1:
+            out[k] = zn[0]
+        elif i >= xn.size:
+            out[k] = zn[-1]
+        else:
+            w = min(1.0, max(0.0, (px - xn[i - 1]) / dx))
+            out[k] = (1.0 - w) * zn[i - 1] + w * zn[i]
+    return out
+
+
+def model_from_files(smesh: str, sed: str, moho: str, geom: str | None = None,
+                     name: str = "") -> tuple[SmeshModel, dict | None]:
+    """The model descriptor (and picks) from the reference's input files:
+    the velocity mesh, the sediment base and the Moho (each interpolated onto
+    the mesh's x) and, optionally, the geometry file (picks = OBS index,
+    phase, shot x, shot z; the geometry dict carries t_obs and uncertainty)."""
+    sm = read_smesh(smesh)
+    xs, zs = read_refl(sed)
+    xm, zm = read_refl(moho)
+    g = read_geom(geom) if geom else None
+    obs_x = g["obs_x"] if g else np.zeros(0)
+    picks = (np.stack([g["obs_id"] - 1, g["phase"], g["rec_x"], g["rec_z"]], axis=1)
+             .astype(np.float64) if g else np.zeros((0, 4)))
+    m = SmeshModel(xpos=sm["xpos"], topo=sm["topo"], zrel=sm["zrel"], vel=sm["vel"],
+                   vwater=sm["vwater"], sed_z=iface_on_grid(xs, zs, sm["xpos"]),
+                   moho_z=iface_on_grid(xm, zm, sm["xpos"]), obs_x=obs_x, picks=picks, name=name)
+    return m, g

@@ -138,6 +138,27 @@ FMT2D_API int fmt2d_select_data(int npick, const int* phase, const double* obs,
                                 int* gindx_out, double* gval_out, double* residual,
                                 double* data_wt, int* pick_of_row);
 
+/* Readers of the reference's input files (read_tomo2d.f90), with Fortran
+ * list-directed input rules (each READ starts a new line and may continue
+ * over lines; blanks or commas between values; D exponents; r*v repeats).
+ * Host only, no context; on error the message is in fmt2d_io_last_error.
+ * Call with NULL arrays first to get the sizes.
+ *
+ * read_smesh (:8-81): header nx nz vwater vair, then xpos[nx], topo[nx],
+ * zpos_rel[nz], then one record of nz velocities per ix; vel is returned
+ * ix fastest (vel[iz*nx + ix]), the layout of fmt2d_model_desc. */
+FMT2D_API int fmt2d_read_smesh(const char* path, int* nx, int* nz, double* vwater, double* vair,
+                               double* xpos, double* topo, double* zrel, double* vel);
+/* read_refl (:83-139): one "x z" pair per line, blank and malformed lines
+ * skipped. */
+FMT2D_API int fmt2d_read_refl(const char* path, int* n, double* x, double* z);
+/* read_geom (:141-248): nobs, then per OBS "tag x z nrec" and nrec lines
+ * "tag x z phase t_obs uncertainty"; obs_id is 1-based. */
+FMT2D_API int fmt2d_read_geom(const char* path, int* nobs, int* nrec, double* obs_x,
+                              double* obs_z, double* rec_x, double* rec_z, int* obs_id,
+                              int* phase, double* t_obs, double* unc);
+FMT2D_API int fmt2d_io_last_error(char* buf, int len);
+
 /* Gaussian smoothing matrix of run_lsqr's smooth_type 2/3 layouts, built on
  * the host (works on a host-only context): which 0 = R_h and 1 = R_v over the
  * velocity parameters (build_gauss_smooth_matrix, src/inversion2d.f90:
