@@ -66,7 +66,7 @@ def lib():
     L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
-    L.fmt2d_set_schedule.argtypes = [V, C.c_int, C.c_double, C.c_int]
+    L.fmt2d_set_schedule.argtypes = [V, C.c_double, C.c_int]
     L.fmt2d_read_smesh.argtypes = [C.c_char_p, P(C.c_int), P(C.c_int), P(C.c_double),
                                    P(C.c_double)] + [C.c_void_p] * 4
     L.fmt2d_read_refl.argtypes = [C.c_char_p, P(C.c_int), C.c_void_p, C.c_void_p]

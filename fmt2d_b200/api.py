@@ -208,8 +208,8 @@ class Fmt2d:
                     "fmt2d_get_field")
         return T, gx, gz
 
-    STATS = ("steps", "batches", "checks", "passed", "solve_ms", "launches", "nodes",
-             "evals", "graphs", "capped", "writes", "unsettled")
+    STATS = ("steps", "batches", "passes", "passed", "solve_ms", "launches", "nodes",
+             "evals", "steps_all", "capped", "writes", "unsettled")
 
     def stats(self) -> dict:
         """Counters of the last forward (fmt2d_stats)."""
@@ -317,12 +317,13 @@ class Fmt2d:
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
 
-    def set_schedule(self, inner: int = 1, window_cells: float = 0.5, steps_per_check: int = 24):
+    def set_schedule(self, window_cells: float = 0.5, max_passes: int = 6):
         """Eikonal solve schedule (fmt2d_set_schedule).  The time window bounds
         how far ahead of the settled times a node may be written; the default
-        (0.5 cells) is the one the parity tests use."""
-        self._check(self.L.fmt2d_set_schedule(self.h, int(inner), float(window_cells),
-                                              int(steps_per_check)), "fmt2d_set_schedule")
+        (0.5 cells) is the one the parity tests use.  max_passes bounds the
+        solve passes (each ends in a fixed-point check of every node)."""
+        self._check(self.L.fmt2d_set_schedule(self.h, float(window_cells), int(max_passes)),
+                    "fmt2d_set_schedule")
         return self
 
     def stream(self) -> int:

@@ -231,7 +231,8 @@ int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask)
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
   const std::string e = ctx->eng->forward(src_x, nsrc, phase_mask);
-  if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  if (!e.empty())
+    return ctx->fail(ctx->eng->not_converged() ? FMT2D_ERR_CONVERGE : FMT2D_ERR_CUDA, e);
   return FMT2D_OK;
 }
 
@@ -251,9 +252,9 @@ int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
   if (!ctx->need_gpu(code)) return code;
   const fmt2d::SolveStats& s = ctx->eng->stats();
   const double v[FMT2D_N_STATS] = {
-      (double)s.rounds,  (double)s.batches, (double)s.final_passes, (double)s.passed,
-      s.round_ms,        (double)s.launches, (double)s.nodes,       (double)s.evals,
-      (double)s.graphs,  (double)s.capped,  (double)s.writes,       (double)s.unsettled};
+      (double)s.rounds,    (double)s.batches, (double)s.final_passes, (double)s.passed,
+      s.round_ms,          (double)s.launches, (double)s.nodes,       (double)s.evals,
+      (double)s.steps_sum, (double)s.capped,  (double)s.writes,       (double)s.unsettled};
   for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
   return FMT2D_OK;
 }
@@ -388,15 +389,13 @@ int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
   return FMT2D_OK;
 }
 
-int fmt2d_set_schedule(fmt2d_ctx* ctx, int inner, double window_cells, int steps_per_check) {
-  if (!ctx || inner < 1 || inner > 64 || !(window_cells > 0.0) || steps_per_check < 1 ||
-      steps_per_check > 256)
+int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes) {
+  if (!ctx || !(window_cells > 0.0) || window_cells > 64.0 || max_passes < 1 || max_passes > 64)
     return FMT2D_ERR_ARG;
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
-  ctx->eng->inner = inner;
   ctx->eng->window_cells = window_cells;
-  ctx->eng->steps_per_check = steps_per_check;
+  ctx->eng->max_passes = max_passes;
   return FMT2D_OK;
 }
 

@@ -1,4 +1,4 @@
-// FP64 tiled eikonal solver: device data of the fields being solved and the
+// FP64 eikonal solver: device data of the fields being solved and the
 // kernels that seed, solve and post-process them.
 //
 // Times and gradients are FP64 on the device so that every candidate time is
@@ -17,7 +17,7 @@ constexpr double kHugeD = 1.0e20;     // mod_fmt2d.f90:616 huge_time
 constexpr double kReachD = 1.0e19;    // a time below this is reached
 constexpr uint8_t kFlSeed = 1, kFlCopy = 2, kFlSusp = 4;
 
-// One time field being solved (static region data plus state).
+// One time field being solved (static region data, state and solver scratch).
 struct Fld64 {
   const uint32_t* code = nullptr;   // per slot (model.h bits)
   const double* vel = nullptr;      // per slot, FP64
@@ -31,9 +31,22 @@ struct Fld64 {
   double2* Gout = nullptr;          // per slot: final gradient (suspect nodes refitted)
   uint8_t* fl = nullptr;            // per slot: kFlSeed | kFlCopy | kFlSusp
   double4* seed = nullptr;          // per slot: seeded (T, gx, gz, -)
-  double* clock = nullptr;          // [0] window end, [1] window step, [2] changed this step
+  double* clock = nullptr;          // [0] window end, [1] window step
   int frozen_slot = -1;             // node fixed at the source (never a trigger)
-  unsigned gbase = 0;               // global id of slot 0 (ids of a batch are contiguous)
+  // solver scratch (per slot unless stated)
+  double* Tn = nullptr;             // new time staged by the evaluation phase
+  double2* Gn = nullptr;            // new gradient staged
+  uint8_t* fln = nullptr;           // new flags staged
+  double* pend = nullptr;           // time a deferred node waits with (< 0: none)
+  unsigned* list_in = nullptr;      // nodes to start from (seeds, re-listed nodes)
+  unsigned* over = nullptr;         // 3*nslots: list overflow (two lists) and commit overflow
+  unsigned* inq = nullptr;          // bitset over slots: listed (when not in shared memory)
+  unsigned* cnt = nullptr;          // [0] list_in length, [1] unsettled nodes found by a check,
+                                    // [2] error (1: step cap), [3] steps of the last solve
+#if defined(__CUDACC__)
+  __host__ __device__
+#endif
+  int nslots() const { return (H + 2) * pitch; }
 };
 
 // Interface data used by the seeding of a stage (FP64, nx nodes).
@@ -57,24 +70,28 @@ struct Seed64 {
   int dst_side = 0, reflect = 0, target_side = 0;
 };
 
+// Solver counters summed over a batch: evaluations, committed writes that
+// changed a node, deferred nodes passed over, steps (summed over fields),
+// largest step count of one field.
+enum { kCtrEval = 0, kCtrWrite, kCtrPass, kCtrSteps, kCtrMaxSteps, kCtrN };
+
 void e64_fill(Fld64* f, int nf, size_t max_slots, cudaStream_t st);
 void e64_init_source(Fld64* f, const double* sx, const double* sz, int nf, cudaStream_t st);
 void e64_seed_iface(Fld64* f, const Seed64* d, int nd, int nx, cudaStream_t st);
-// List every seeded node and its neighbours (list/cnt), set the windows.
-void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, unsigned* list,
-               unsigned* cnt, unsigned* inq, cudaStream_t st);
-// One step over the list `in` (see k_step); ver / pend: per node input
-// version and deferred-time record, zeroed at the start of a batch.
-void e64_step(Fld64* f, int nf, const unsigned* in, const unsigned* in_cnt, unsigned* out,
-              unsigned* out_cnt, unsigned* zero_cnt, unsigned* inq, unsigned* done, unsigned* ver,
-              unsigned long long* pend, int grid, unsigned long long* ctr, cudaStream_t st);
-void e64_verify(Fld64* f, int nf, size_t max_slots, unsigned* list, unsigned* cnt, unsigned* inq,
-                unsigned* bad, cudaStream_t st);
+// List every seeded node and its neighbours in list_in; set the windows.
+void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, cudaStream_t st);
+// Solve every field of the batch from its list_in (one thread block per
+// field, all steps in one launch).  max_steps bounds the steps of a field;
+// a field that reaches it sets cnt[2] = 1.
+void e64_solve(Fld64* f, int nf, size_t max_slots, long long max_steps, unsigned long long* ctr,
+               cudaStream_t st);
+// Fixed-point check of every node: a node whose evaluation would change it
+// is listed in list_in and counted in cnt[1].
+void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st);
 void e64_finish(Fld64* f, int nf, size_t max_slots, const int* water_up, cudaStream_t st);
 void e64_headwave(Fld64* f, const int* hw_slot, const double* hw_v, double dx_if, int nx,
                   double* scratch, const int* which, int nsel, cudaStream_t st);
 void e64_export(const double* T, const double2* G, const int* slot_of_node, int nnode, double* oT,
                 double* ogx, double* ogz, cudaStream_t st);
-int e64_step_grid(int device);
 
 }  // namespace fmt2d

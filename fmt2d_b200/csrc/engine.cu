@@ -86,7 +86,6 @@ Engine::Engine(int device) : device_(device) {
   cudaSetDevice(device_);
   cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
   cudaMallocHost(&h_count_, 4 * sizeof(unsigned));
-  step_grid_ = e64_step_grid(device_);
 }
 
 Engine::~Engine() {
@@ -215,6 +214,7 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
     }
   }
   stats_ = SolveStats();
+  not_converged_ = false;
   for (int level = 0; level <= 3; ++level) {
     std::vector<std::pair<int, int>> items;
     for (int tf = 1; tf <= 12; ++tf)
@@ -262,42 +262,54 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   std::vector<double> wstep(nf);
   size_t total = 0, max_slots = 0;
   for (int i = 0; i < nf; ++i) {
+    const int tf = items[i].second;
+    const DevRegionStore& D = reg_[kTf[tf].reg];
+    total += D.nslots;
+    max_slots = std::max(max_slots, D.nslots);
+  }
+  if (total >= 0x7fffffffull) return "batch too large for 31-bit slot ids";
+  // solver scratch of the batch, per slot: staged time, gradient and flags,
+  // pending time, start list, list and commit overflow, listed bitset
+  const size_t words = (total + 31 * (size_t)nf + 31) / 32 + (size_t)nf;
+  d_sTn_.alloc(total * sizeof(double));
+  d_sGn_.alloc(total * sizeof(double2));
+  d_sfln_.alloc(total);
+  d_spend_.alloc(total * sizeof(double));
+  d_slist_.alloc(total * sizeof(unsigned));
+  d_sover_.alloc(3 * total * sizeof(unsigned));
+  d_sinq_.alloc(words * sizeof(unsigned));
+  d_scnt_.alloc((size_t)nf * 4 * sizeof(unsigned));
+  d_ctr_.alloc(kCtrN * sizeof(unsigned long long));
+  if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_slist_.p || !d_sover_.p ||
+      !d_sinq_.p || !d_scnt_.p || !d_ctr_.p)
+    return "device allocation failed for the solver scratch";
+  size_t base = 0, wbase = 0;
+  for (int i = 0; i < nf; ++i) {
     const int s = items[i].first, tf = items[i].second;
     const DevRegionStore& D = reg_[kTf[tf].reg];
     hf[i] = field_view(s, tf);
-    hf[i].gbase = (unsigned)total;
-    total += D.nslots;
-    max_slots = std::max(max_slots, D.nslots);
+    hf[i].Tn = d_sTn_.as<double>() + base;
+    hf[i].Gn = d_sGn_.as<double2>() + base;
+    hf[i].fln = d_sfln_.as<uint8_t>() + base;
+    hf[i].pend = d_spend_.as<double>() + base;
+    hf[i].list_in = d_slist_.as<unsigned>() + base;
+    hf[i].over = d_sover_.as<unsigned>() + 3 * base;
+    hf[i].inq = d_sinq_.as<unsigned>() + wbase;
+    hf[i].cnt = d_scnt_.as<unsigned>() + 4 * (size_t)i;
+    base += D.nslots;
+    wbase += (D.nslots + 31) / 32;
     up[i] = kTf[tf].water_up;
     wstep[i] = window_cells * m_.dx / D.vmax;
     if (tf == 5) hw.push_back(i);
   }
-  if (total >= 0xffffffffull) return "batch too large for 32-bit node ids";
   std::string e;
   if (!(e = put(d_fields_, hf, stream_)).empty()) return e;
   if (!(e = put(d_up_, up, stream_)).empty()) return e;
   if (!(e = put(d_step_, wstep, stream_)).empty()) return e;
-  // three lists (read, written, emptied) rotate through the steps
-  d_list_.alloc(3 * total * sizeof(unsigned));
-  d_inq_.alloc(((total + 31) / 32) * sizeof(unsigned));
-  d_count_.alloc(8 * sizeof(unsigned));
-  d_done_.alloc(16);
-  d_ctr_.alloc(8 * sizeof(unsigned long long));
-  d_ver_.alloc(total * sizeof(unsigned));
-  d_pend_.alloc(total * sizeof(unsigned long long));
-  if (!d_list_.p || !d_inq_.p || !d_count_.p || !d_done_.p || !d_ctr_.p || !d_ver_.p ||
-      !d_pend_.p)
-    return "device allocation failed for the active lists";
-  unsigned* L[3] = {d_list_.as<unsigned>(), d_list_.as<unsigned>() + total,
-                    d_list_.as<unsigned>() + 2 * total};
-  unsigned* cnt = d_count_.as<unsigned>();    // [0..2] list lengths, [3] check result
   unsigned long long* dctr = d_ctr_.as<unsigned long long>();
-  CK(cudaMemsetAsync(d_inq_.p, 0, ((total + 31) / 32) * sizeof(unsigned), stream_));
-  CK(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned), stream_));
-  CK(cudaMemsetAsync(d_done_.p, 0, 16, stream_));
-  CK(cudaMemsetAsync(dctr, 0, 8 * sizeof(unsigned long long), stream_));
-  CK(cudaMemsetAsync(d_ver_.p, 0, total * sizeof(unsigned), stream_));
-  CK(cudaMemsetAsync(d_pend_.p, 0, total * sizeof(unsigned long long), stream_));
+  CK(cudaMemsetAsync(d_sinq_.p, 0, words * sizeof(unsigned), stream_));
+  CK(cudaMemsetAsync(d_scnt_.p, 0, (size_t)nf * 4 * sizeof(unsigned), stream_));
+  CK(cudaMemsetAsync(dctr, 0, kCtrN * sizeof(unsigned long long), stream_));
   Fld64* dF = d_fields_.as<Fld64>();
   e64_fill(dF, nf, max_slots, stream_);
   ++stats_.launches;
@@ -336,62 +348,44 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     e64_seed_iface(dF, d_seeds_.as<Seed64>(), nf, m_.nx, stream_);
     ++stats_.launches;
   }
-  e64_start(dF, nf, max_slots, d_step_.as<double>(), L[0], cnt + 0, d_inq_.as<unsigned>(),
-            stream_);
+  e64_start(dF, nf, max_slots, d_step_.as<double>(), stream_);
   stats_.launches += 2;
   CK(cudaGetLastError());
-  // the step loop: graphs of steps_per_check steps (a multiple of 3, so every
-  // graph starts reading list 0), then the length of list 0 comes back
-  const int spc = std::max(3, steps_per_check / 3 * 3);
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-  for (int k = 0; k < spc; ++k) {
-    const int a = k % 3, b = (k + 1) % 3, c = (k + 2) % 3;
-    e64_step(dF, nf, L[a], cnt + a, L[b], cnt + b, cnt + c, d_inq_.as<unsigned>(),
-             d_done_.as<unsigned>(), d_ver_.as<unsigned>(), d_pend_.as<unsigned long long>(),
-             step_grid_, dctr, stream_);
+  // solve, then check every node; nodes the check re-lists are solved again
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return "cudaEventCreate failed";
   }
-  CK(cudaMemcpyAsync(h_count_, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamEndCapture(stream_, &graph));
-  CK(cudaGraphInstantiate(&exec, graph, 0));
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, stream_);
-  long long steps = 0, steps_at_check = 0;
-  int verify_passes = 0;
   std::string err;
-  for (;;) {
-    const cudaError_t ge = cudaGraphLaunch(exec, stream_);
-    if (ge != cudaSuccess) { err = std::string("cudaGraphLaunch: ") + cudaGetErrorString(ge); break; }
-    steps += spc;
-    stats_.launches += spc;
-    const cudaError_t se = cudaStreamSynchronize(stream_);
-    if (se != cudaSuccess) { err = std::string("step loop: ") + cudaGetErrorString(se); break; }
-    if (h_count_[0] != 0u) {
-      // after a fixed-point check no node is final, so what still moves
-      // gets a bounded number of steps and is reported in the stats
-      if (verify_passes > 0 && steps - steps_at_check >= check_steps) {
-        stats_.capped += h_count_[0];
-        break;
-      }
-      if (steps >= max_steps) { err = "eikonal solve did not converge within the step cap"; break; }
-      continue;
-    }
-    // empty list: check the fixed point of every node, resume if needed
-    if (verify_passes >= 6) break;   // nodes still moving are reported in the stats
-    ++verify_passes;
-    ++stats_.final_passes;
-    cudaMemsetAsync(cnt + 3, 0, sizeof(unsigned), stream_);
-    e64_verify(dF, nf, max_slots, L[0], cnt + 0, d_inq_.as<unsigned>(), cnt + 3, stream_);
+  std::vector<unsigned> hc((size_t)nf * 4);
+  cudaEventRecord(e0, stream_);
+  unsigned long long bad = 0;
+  for (int pass = 0;; ++pass) {
+    e64_solve(dF, nf, max_slots, max_steps, dctr, stream_);
     ++stats_.launches;
-    cudaMemcpyAsync(h_count_, cnt + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_);
-    const cudaError_t ve = cudaStreamSynchronize(stream_);
-    if (ve != cudaSuccess) { err = std::string("fixed-point check: ") + cudaGetErrorString(ve); break; }
-    steps_at_check = steps;
-    if (h_count_[0] == 0u) break;
-    stats_.unsettled = h_count_[0];
+    ++stats_.final_passes;
+    cudaMemsetAsync(d_sinq_.p, 0, words * sizeof(unsigned), stream_);
+    e64_verify(dF, nf, max_slots, stream_);
+    ++stats_.launches;
+    cudaError_t ce = cudaMemcpyAsync(hc.data(), d_scnt_.p, hc.size() * sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost, stream_);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream_);
+    if (ce != cudaSuccess) { err = std::string("eikonal solve: ") + cudaGetErrorString(ce); break; }
+    bad = 0;
+    unsigned capped = 0;
+    for (int i = 0; i < nf; ++i) {
+      bad += hc[4 * (size_t)i + 1];
+      capped += hc[4 * (size_t)i + 2];
+    }
+    if (capped) {
+      stats_.capped += capped;
+      not_converged_ = true;
+      err = "eikonal solve reached its step cap in " + std::to_string(capped) + " fields";
+      break;
+    }
+    if (bad == 0 || pass + 1 >= max_passes) break;
   }
   cudaEventRecord(e1, stream_);
   cudaEventSynchronize(e1);
@@ -399,18 +393,22 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
   if (!err.empty()) return err;
   stats_.round_ms += ms;
-  stats_.rounds += steps;
   {
-    unsigned long long c[3];
+    unsigned long long c[kCtrN];
     CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
-    stats_.evals += c[0];
-    stats_.writes += c[1];
-    stats_.passed += c[2];
-    stats_.graphs += steps / spc;
+    stats_.evals += c[kCtrEval];
+    stats_.writes += c[kCtrWrite];
+    stats_.passed += c[kCtrPass];
+    stats_.rounds += (long long)c[kCtrMaxSteps];
+    stats_.steps_sum += c[kCtrSteps];
+  }
+  if (bad) {
+    stats_.unsettled += bad;
+    not_converged_ = true;
+    return "eikonal solve did not reach its fixed point (" + std::to_string(bad) +
+           " nodes still move after " + std::to_string(max_passes) + " passes)";
   }
   e64_finish(dF, nf, max_slots, d_up_.as<int>(), stream_);
   stats_.launches += 2;

@@ -44,13 +44,13 @@ struct FieldStore {
 };
 
 struct SolveStats {
-  long long rounds = 0;       // step kernels run
-  int batches = 0, final_passes = 0;   // stage batches; fixed-point checks
+  long long rounds = 0;       // steps of the longest field solve, summed over batches
+  unsigned long long steps_sum = 0;   // steps summed over every field
+  int batches = 0, final_passes = 0;   // stage batches; solve passes (each ends in a fixed-point check)
   double round_ms = 0.0;      // device time of the step loops
   unsigned long long evals = 0, writes = 0, passed = 0;   // node evaluations; writes; deferred nodes passed over
-  unsigned long long graphs = 0;      // captured step graphs launched
   unsigned long long unsettled = 0;   // nodes the last fixed-point check re-listed
-  unsigned long long capped = 0;      // nodes still moving when the steps after a check ran out
+  unsigned long long capped = 0;      // fields that reached the step cap
   long long launches = 0;     // kernels launched since the last forward began
   long long nodes = 0;        // region nodes of the time fields solved
 };
@@ -76,11 +76,11 @@ class Engine {
   const Model& model() const { return m_; }
   cudaStream_t stream() const { return stream_; }
   const SolveStats& stats() const { return stats_; }
-  int inner = 1;             // unused by the list schedule (kept for the C ABI)
+  // the last forward failed because a field did not reach its fixed point
+  bool not_converged() const { return not_converged_; }
   double window_cells = 0.5; // window step: this many cells at the region's largest velocity
-  int steps_per_check = 24;  // steps per captured graph between list checks (multiple of 3)
-  long long max_steps = 2000000;  // safety cap on steps per level
-  long long check_steps = 4096;   // steps allowed after each fixed-point check
+  long long max_steps = 4000000;  // safety cap on the steps of one field's solve
+  int max_passes = 6;             // solve passes (each followed by a check of every node)
   // device pointers of a solved field (FP64 time, double2 final gradient per slot)
   const double* field_t(int src, int tf) const { return fields_[src][tf].T.as<double>(); }
   const double2* field_g(int src, int tf) const { return fields_[src][tf].Gout.as<double2>(); }
@@ -103,16 +103,16 @@ class Engine {
   DevBuf hw_slot_, hw_v_;
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
-  DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_count_, d_scratch_, d_which_, d_up_, d_step_,
-      d_done_, d_ctr_, d_list_, d_inq_, d_ver_, d_pend_;
+  DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_scratch_, d_which_, d_up_, d_step_, d_ctr_;
+  DevBuf d_sTn_, d_sGn_, d_sfln_, d_spend_, d_slist_, d_sover_, d_sinq_, d_scnt_;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
       d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
   int npick_ = -1, rows_ = 0;
   long long nnz_ = 0;
   double trace_ms_ = 0.0;
   unsigned* h_count_ = nullptr;
-  int step_grid_ = 1;
   SolveStats stats_;
+  bool not_converged_ = false;
 };
 
 }  // namespace fmt2d

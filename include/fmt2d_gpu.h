@@ -51,6 +51,7 @@ extern "C" {
 #define FMT2D_ERR_CUDA (-2)     /* CUDA runtime failure or no device */
 #define FMT2D_ERR_STATE (-3)    /* call out of order (e.g. no model uploaded) */
 #define FMT2D_ERR_MODEL (-4)    /* model rejected by the geometry build */
+#define FMT2D_ERR_CONVERGE (-5) /* eikonal solve did not reach its fixed point */
 
 typedef struct fmt2d_ctx fmt2d_ctx;
 
@@ -179,13 +180,14 @@ FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int p
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
 /* Counters of the last fmt2d_forward (and of the exports since), in this
- * order: [0] step kernels, [1] stage batches, [2] fixed-point checks,
- * [3] deferred nodes passed over without evaluation, [4] device milliseconds
- * of the step loops, [5] kernel launches, [6] region nodes of the solved time
- * fields, [7] node evaluations, [8] step graphs launched, [9] nodes still
- * moving when the steps allowed after a fixed-point check ran out (0 when
- * every field reached its fixed point), [10] node writes, [11] nodes the
- * last fixed-point check re-listed.
+ * order: [0] steps of the longest field solve, summed over stage levels,
+ * [1] stage levels, [2] solve passes (each ends in a fixed-point check of
+ * every node), [3] deferred nodes passed over without evaluation, [4] device
+ * milliseconds of the solves and checks, [5] kernel launches, [6] region nodes
+ * of the solved time fields, [7] node evaluations, [8] steps summed over all
+ * fields, [9] fields that reached the step cap, [10] node writes that changed
+ * a node, [11] nodes the last fixed-point check found still moving (nonzero
+ * only when fmt2d_forward returned FMT2D_ERR_CONVERGE).
  * Writes min(n, FMT2D_N_STATS) values.  No reference counterpart (diagnostics). */
 #define FMT2D_N_STATS 12
 FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
@@ -266,14 +268,14 @@ FMT2D_API int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params
 FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* Schedule of the eikonal solve (no reference counterpart; the reference's
- * heap has no schedule): `inner` is accepted for compatibility and unused
- * (1..64), the time window's step in cells at the region's largest velocity
- * (> 0, default 0.5), and steps between convergence checks (1..256).  The
- * window bounds how far ahead of the settled times a node may be written:
- * wider windows reach fixed points that can differ from the heap's order and
- * take more steps per window; the default is the one the parity tests use. */
-FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, int inner, double window_cells,
-                                 int steps_per_check);
+ * heap has no schedule): the time window's step in cells at the region's
+ * largest velocity (0 < window_cells <= 64, default 0.5) and the number of
+ * solve passes, each followed by a fixed-point check of every node
+ * (1..64, default 6); a forward whose last check still finds nodes that
+ * move returns FMT2D_ERR_CONVERGE.  The window bounds how far ahead of the
+ * settled times a node may be written; the default is the one the parity
+ * tests use. */
+FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes);
 
 /* The CUDA stream (cudaStream_t) all work of the context is issued on, for
  * callers that record events around fmt2d_forward.  No reference counterpart. */
