@@ -39,17 +39,22 @@ using namespace ev;
 
 // ---------------------------------------------------------------- field solve
 constexpr int kSolveThreads = 256;
+constexpr int kSolveWarps = kSolveThreads / 32;
 constexpr unsigned kLCap = 4096;          // entries of each list held in shared memory
 constexpr unsigned kCCap = 2048;          // commit entries held in shared memory
-constexpr int kSmemBitsMax = 24 * 1024;   // bitset words kept in shared memory (786,432 slots)
+constexpr int kTileRows = 8;              // a tile: 8 slot rows x 32 slot columns (one bitset word per row)
+constexpr int kTilesMax = 12288;          // tiles per field (tile minima live in shared memory)
+constexpr size_t kSmemMax = 227 * 1024;   // dynamic shared memory of the solve block
 constexpr unsigned kSpreadBit = 0x80000000u;
+constexpr unsigned long long kNone = ULLONG_MAX;
 
 struct SolveShared {
   Fld64 F;
   unsigned cnt[2];                 // list lengths
   unsigned nc[2];                  // commit list length, by step parity
   int changed[2];                  // a committed write moved a node, by step parity
-  unsigned long long minpend[2];   // smallest pending time (bits of a positive double)
+  unsigned nready[2];              // tiles to release, by release parity
+  unsigned long long gmin[2];      // earliest waiting time (bits of a positive double)
   int err;
 };
 
@@ -71,33 +76,61 @@ __device__ __forceinline__ unsigned long long dbits(double d) {
   return (unsigned long long)__double_as_longlong(d);
 }
 
+__host__ __device__ inline int tiles_of(const Fld64& F) {
+  return ((F.H + 2 + kTileRows - 1) / kTileRows) * (F.pitch / 32);
+}
+
 // Solve every field of the batch from its list_in (one block per field).
-// smem_bits: bitset words available in shared memory; a field whose bitset
-// is larger uses its global one.
+//
+// Waiting nodes: a node whose new time lies beyond the window records it in
+// pend and sets its bit in the waiting bitset; each tile of 8 x 32 slots
+// keeps the smallest waiting time of its nodes.  When the window moves on,
+// the tiles it has reached are scanned (a warp per tile) and their nodes
+// that are due are listed, so a waiting node costs nothing until then.  A
+// waiting node whose input changes is listed at once (its recorded time was
+// computed from the old value).
+//
+// Shared memory: the two lists, the commit list, the tile minima and the
+// list of tiles to scan, and (when they fit) the listed and waiting bitsets;
+// smem_bits is the bitset size in words that fits, larger fields use their
+// global bitsets.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_solve(Fld64* fields, int nf, int smem_bits, long long max_steps,
+    k_solve(Fld64* fields, int nf, int smem_bits, int tiles_cap, long long max_steps,
             unsigned long long* ctr) {
-  extern __shared__ unsigned dsm[];
+  extern __shared__ __align__(16) unsigned char dsm_raw[];
   __shared__ SolveShared sh;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     sh.F = fields[blockIdx.x];
     sh.cnt[0] = sh.cnt[1] = 0u;
     sh.nc[0] = sh.nc[1] = 0u;
     sh.changed[0] = sh.changed[1] = 0;
-    sh.minpend[0] = sh.minpend[1] = ULLONG_MAX;
+    sh.nready[0] = sh.nready[1] = 0u;
+    sh.gmin[0] = sh.gmin[1] = kNone;
     sh.err = 0;
   }
   __syncthreads();
   const Fld64& F = sh.F;
   const unsigned ns = (unsigned)F.nslots();
   const unsigned nbw = (ns + 31u) >> 5;
-  unsigned* sl[2] = {dsm, dsm + kLCap};
-  unsigned* scl = dsm + 2 * kLCap;
-  unsigned* bits = nbw <= (unsigned)smem_bits ? dsm + 2 * kLCap + kCCap : F.inq;
+  const int tcols = F.pitch / 32, ntiles = tiles_of(F);
+  unsigned long long* tmin = reinterpret_cast<unsigned long long*>(dsm_raw);
+  unsigned* sl[2];
+  sl[0] = reinterpret_cast<unsigned*>(tmin + tiles_cap);
+  sl[1] = sl[0] + kLCap;
+  unsigned* scl = sl[1] + kLCap;
+  unsigned short* ready = reinterpret_cast<unsigned short*>(scl + kCCap);
+  unsigned* sbits = reinterpret_cast<unsigned*>(ready + tiles_cap);
+  const bool local_bits = nbw <= (unsigned)smem_bits;
+  unsigned* bits = local_bits ? sbits : F.inq;
+  unsigned* wbits = local_bits ? sbits + smem_bits : F.wait;
   unsigned* ov[2] = {F.over, F.over + ns};
   unsigned* cov = F.over + 2 * (size_t)ns;
-  for (unsigned w = tid; w < nbw; w += kSolveThreads) bits[w] = 0u;
+  for (unsigned w = tid; w < nbw; w += kSolveThreads) {
+    bits[w] = 0u;
+    wbits[w] = 0u;
+  }
+  for (int t = tid; t < ntiles; t += kSolveThreads) tmin[t] = kNone;
   __syncthreads();
   {
     const unsigned n0 = F.cnt[0];
@@ -107,8 +140,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __syncthreads();
   double W = F.clock[0];
   const double wstep = F.clock[1];
-  unsigned long long n_eval = 0, n_write = 0, n_pass = 0;
-  int cur = 0;
+  unsigned long long n_eval = 0, n_write = 0, n_rel = 0;
+  int cur = 0, rp = 0;
   long long it = 0;
   for (;; ++it) {
     const unsigned n = sh.cnt[cur];
@@ -122,13 +155,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     for (unsigned i = tid; i < n; i += kSolveThreads) {
       const unsigned s = get_entry(sl[cur], ov[cur], i);
       atomicAnd(bits + (s >> 5), ~(1u << (s & 31)));
-      const double pd = F.pend[s];
-      if (pd > W) {   // still beyond the window, inputs unchanged
-        push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
-        atomicMin(&sh.minpend[par], dbits(pd));
-        ++n_pass;
-        continue;
-      }
       const NewV nv = evaluate(F, (int)s);
       ++n_eval;
       if (!nv.write) {
@@ -137,8 +163,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       }
       if (nv.T < kReachD && nv.T > W) {   // beyond the window: wait for it
         F.pend[s] = nv.T;
-        push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
-        atomicMin(&sh.minpend[par], dbits(nv.T));
+        atomicOr(wbits + (s >> 5), 1u << (s & 31));
+        const int row = (int)(s / (unsigned)F.pitch), col = (int)(s - (unsigned)row * F.pitch);
+        atomicMin(tmin + (row / kTileRows) * tcols + (col >> 5), dbits(nv.T));
         continue;
       }
       F.pend[s] = -1.0;
@@ -161,7 +188,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       sh.cnt[cur] = 0u;
       sh.nc[par ^ 1] = 0u;
       sh.changed[par ^ 1] = 0;
-      sh.minpend[par ^ 1] = ULLONG_MAX;
     }
     for (unsigned j = tid; j < nc; j += kSolveThreads) {
       const unsigned s = (j < kCCap ? scl[j] : cov[j - kCCap]) & ~kSpreadBit;
@@ -174,8 +200,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     __syncthreads();
     // spread: every candidate of a node u that involves node v is at or above
     // v's time, so a change of v from a to b can only move nodes at or above
-    // min(a, b); those below are not listed, but any time they wait with is
-    // dropped (it was computed from the old value)
+    // min(a, b); those below are not listed unless they wait with a time
+    // computed from the old value, which is dropped
     for (unsigned j = tid; j < nc; j += kSolveThreads) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
       if (!(e & kSpreadBit)) continue;
@@ -184,21 +210,71 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       int t[16];
       const int k = spread_targets(F, s, t);
       for (int q = 0; q < k; ++q) {
+        const bool waiting = F.pend[t[q]] >= 0.0;
         F.pend[t[q]] = -1.0;
-        if (!(F.T[t[q]] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t[q]);
+        if (waiting || !(F.T[t[q]] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t[q]);
       }
     }
     __syncthreads();
-    // the window moves on after a step that changed nothing inside it,
-    // straight to the earliest waiting time when that lies further on
-    if (!sh.changed[par]) {
-      double w2 = W + wstep;
-      const unsigned long long mp = sh.minpend[par];
-      if (mp != ULLONG_MAX) {
-        const double md = __longlong_as_double((long long)mp);
-        if (md > w2) w2 = md;
+    // the window moves on after a step that changed nothing inside it (or
+    // listed nothing); the tiles it reaches release their due nodes, and when
+    // none is due it jumps to the earliest waiting time
+    const bool chg = sh.changed[par] != 0;
+    if (!chg || sh.cnt[nxt] == 0u) {
+      if (!chg) W += wstep;
+      for (;;) {
+        const int q = rp & 1;
+        ++rp;
+        for (int t = tid; t < ntiles; t += kSolveThreads)
+          if (tmin[t] != kNone && __longlong_as_double((long long)tmin[t]) <= W)
+            ready[atomicAdd(&sh.nready[q], 1u)] = (unsigned short)t;
+        __syncthreads();
+        const unsigned nr = sh.nready[q];
+        if (tid == 0) {
+          sh.nready[q ^ 1] = 0u;
+          sh.gmin[q ^ 1] = kNone;
+        }
+        for (unsigned k = warp; k < nr; k += kSolveWarps) {
+          const int t = ready[k];
+          const int r0 = (t / tcols) * kTileRows, c0 = (t % tcols) * 32;
+          unsigned long long m = kNone;
+          for (int rr = 0; rr < kTileRows; ++rr) {
+            const int r = r0 + rr;
+            if (r >= F.H + 2) break;
+            const unsigned w = (unsigned)(r * F.pitch + c0) >> 5;
+            const unsigned word = wbits[w];
+            bool clear = false;
+            if (word & (1u << lane)) {
+              const unsigned s = (unsigned)(r * F.pitch + c0 + lane);
+              const double pd = F.pend[s];
+              if (pd < 0.0) {
+                clear = true;                 // listed since (an input changed)
+              } else if (pd <= W) {
+                clear = true;
+                push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
+                ++n_rel;
+              } else {
+                m = min(m, dbits(pd));
+              }
+            }
+            const unsigned cm = __ballot_sync(0xffffffffu, clear);
+            if (lane == 0 && cm) wbits[w] = word & ~cm;
+          }
+#pragma unroll
+          for (int o = 16; o; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+          if (lane == 0) tmin[t] = m;
+        }
+        __syncthreads();
+        if (sh.cnt[nxt] != 0u) break;
+        // nothing due: the earliest waiting time, if any
+        unsigned long long m = kNone;
+        for (int t = tid; t < ntiles; t += kSolveThreads) m = min(m, tmin[t]);
+        if (m != kNone) atomicMin(&sh.gmin[q], m);
+        __syncthreads();
+        const unsigned long long g = sh.gmin[q];
+        if (g == kNone) break;
+        W = fmax(W, __longlong_as_double((long long)g));
       }
-      W = w2;
     }
     cur = nxt;
   }
@@ -206,12 +282,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   for (int o = 16; o; o >>= 1) {
     n_eval += __shfl_xor_sync(0xffffffffu, n_eval, o);
     n_write += __shfl_xor_sync(0xffffffffu, n_write, o);
-    n_pass += __shfl_xor_sync(0xffffffffu, n_pass, o);
+    n_rel += __shfl_xor_sync(0xffffffffu, n_rel, o);
   }
-  if ((tid & 31) == 0 && ctr) {
+  if (lane == 0 && ctr) {
     atomicAdd(ctr + kCtrEval, n_eval);
     atomicAdd(ctr + kCtrWrite, n_write);
-    atomicAdd(ctr + kCtrPass, n_pass);
+    atomicAdd(ctr + kCtrPass, n_rel);
   }
   __syncthreads();
   if (tid == 0) {
@@ -514,13 +590,29 @@ void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, cudaStrea
   k_queue_seeds<<<dim3(bx, nf), 256, 0, st>>>(f, nf);
   k_clock<<<nf, 256, 0, st>>>(f, nf, step);
 }
-void e64_solve(Fld64* f, int nf, size_t max_slots, long long max_steps, unsigned long long* ctr,
-               cudaStream_t st) {
+// Dynamic shared memory of k_solve for a batch whose largest field has
+// max_slots slots and max_tiles tiles (tiles_cap rounded up to a multiple of
+// 8); smem_bits: words of each bitset kept in shared memory (0: global).
+static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* tiles_cap) {
+  const int cap = (max_tiles + 7) / 8 * 8;
+  const size_t fixed = (size_t)cap * sizeof(unsigned long long) +
+                       (2 * (size_t)kLCap + kCCap) * sizeof(unsigned) +
+                       (size_t)cap * sizeof(unsigned short);
   const size_t nbw = (max_slots + 31) / 32;
-  const int smem_bits = (int)std::min<size_t>(nbw, (size_t)kSmemBitsMax);
-  const size_t bytes = (2 * (size_t)kLCap + kCCap + (size_t)smem_bits) * sizeof(unsigned);
+  const size_t room = fixed + 1024 < kSmemMax ? (kSmemMax - fixed - 1024) / (2 * sizeof(unsigned)) : 0;
+  const size_t words = nbw <= room ? nbw : 0;   // both bitsets of every field fit, or none
+  *smem_bits = (int)words;
+  *tiles_cap = cap;
+  return fixed + 2 * words * sizeof(unsigned);
+}
+int e64_tiles(const Fld64& f) { return tiles_of(f); }
+int e64_tiles_max() { return kTilesMax; }
+void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
+               unsigned long long* ctr, cudaStream_t st) {
+  int smem_bits = 0, cap = 0;
+  const size_t bytes = solve_smem(max_slots, max_tiles, &smem_bits, &cap);
   cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, max_steps, ctr);
+  k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, cap, max_steps, ctr);
 }
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st) {
   const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 512);

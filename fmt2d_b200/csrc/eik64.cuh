@@ -41,6 +41,7 @@ struct Fld64 {
   unsigned* list_in = nullptr;      // nodes to start from (seeds, re-listed nodes)
   unsigned* over = nullptr;         // 3*nslots: list overflow (two lists) and commit overflow
   unsigned* inq = nullptr;          // bitset over slots: listed (when not in shared memory)
+  unsigned* wait = nullptr;         // bitset over slots: waiting (when not in shared memory)
   unsigned* cnt = nullptr;          // [0] list_in length, [1] unsettled nodes found by a check,
                                     // [2] error (1: step cap), [3] steps of the last solve
 #if defined(__CUDACC__)
@@ -71,8 +72,8 @@ struct Seed64 {
 };
 
 // Solver counters summed over a batch: evaluations, committed writes that
-// changed a node, deferred nodes passed over, steps (summed over fields),
-// largest step count of one field.
+// changed a node, waiting nodes released by the window, steps (summed over
+// fields), largest step count of one field.
 enum { kCtrEval = 0, kCtrWrite, kCtrPass, kCtrSteps, kCtrMaxSteps, kCtrN };
 
 void e64_fill(Fld64* f, int nf, size_t max_slots, cudaStream_t st);
@@ -81,10 +82,14 @@ void e64_seed_iface(Fld64* f, const Seed64* d, int nd, int nx, cudaStream_t st);
 // List every seeded node and its neighbours in list_in; set the windows.
 void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, cudaStream_t st);
 // Solve every field of the batch from its list_in (one thread block per
-// field, all steps in one launch).  max_steps bounds the steps of a field;
+// field, all steps in one launch; max_tiles: the most tiles of a field,
+// e64_tiles).  max_steps bounds the steps of a field;
 // a field that reaches it sets cnt[2] = 1.
-void e64_solve(Fld64* f, int nf, size_t max_slots, long long max_steps, unsigned long long* ctr,
-               cudaStream_t st);
+void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
+               unsigned long long* ctr, cudaStream_t st);
+// Tiles of a field's waiting-node index, and the most a field may have.
+int e64_tiles(const Fld64& f);
+int e64_tiles_max();
 // Fixed-point check of every node: a node whose evaluation would change it
 // is listed in list_in and counted in cnt[1].
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st);

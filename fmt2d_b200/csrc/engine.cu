@@ -277,13 +277,14 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   d_spend_.alloc(total * sizeof(double));
   d_slist_.alloc(total * sizeof(unsigned));
   d_sover_.alloc(3 * total * sizeof(unsigned));
-  d_sinq_.alloc(words * sizeof(unsigned));
+  d_sinq_.alloc(2 * words * sizeof(unsigned));
   d_scnt_.alloc((size_t)nf * 4 * sizeof(unsigned));
   d_ctr_.alloc(kCtrN * sizeof(unsigned long long));
   if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_slist_.p || !d_sover_.p ||
       !d_sinq_.p || !d_scnt_.p || !d_ctr_.p)
     return "device allocation failed for the solver scratch";
   size_t base = 0, wbase = 0;
+  int max_tiles = 0;
   for (int i = 0; i < nf; ++i) {
     const int s = items[i].first, tf = items[i].second;
     const DevRegionStore& D = reg_[kTf[tf].reg];
@@ -295,6 +296,9 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     hf[i].list_in = d_slist_.as<unsigned>() + base;
     hf[i].over = d_sover_.as<unsigned>() + 3 * base;
     hf[i].inq = d_sinq_.as<unsigned>() + wbase;
+    hf[i].wait = d_sinq_.as<unsigned>() + words + wbase;
+    if (e64_tiles(hf[i]) > e64_tiles_max()) return "region too large for the eikonal solver";
+    max_tiles = std::max(max_tiles, e64_tiles(hf[i]));
     hf[i].cnt = d_scnt_.as<unsigned>() + 4 * (size_t)i;
     base += D.nslots;
     wbase += (D.nslots + 31) / 32;
@@ -363,7 +367,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   cudaEventRecord(e0, stream_);
   unsigned long long bad = 0;
   for (int pass = 0;; ++pass) {
-    e64_solve(dF, nf, max_slots, max_steps, dctr, stream_);
+    e64_solve(dF, nf, max_slots, max_tiles, max_steps, dctr, stream_);
     ++stats_.launches;
     ++stats_.final_passes;
     cudaMemsetAsync(d_sinq_.p, 0, words * sizeof(unsigned), stream_);
