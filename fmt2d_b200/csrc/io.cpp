@@ -4,13 +4,16 @@
 // Fortran list-directed input: each READ starts at a new line, takes its
 // values from as many lines as it needs (blanks or commas between values,
 // D or E exponents, r*v repeats, a slash ending the record) and drops the
-// rest of its last line.
+// rest of its last line.  Two commas with only blanks between them (or a
+// comma that opens the READ) give a null value, which leaves the Fortran
+// variable unset; the readers report it as an unreadable item.
 #include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -28,7 +31,10 @@ int io_fail(int code, const std::string& msg) {
 // A file read record by record with list-directed value parsing.
 class ListReader {
  public:
-  explicit ListReader(const std::string& path) : in_(path) {}
+  explicit ListReader(const std::string& path)
+      : own_(new std::ifstream(path)), in_(*own_) {}
+  // A reader over text already in memory (one line read with `*` format).
+  explicit ListReader(std::istream& in) : in_(in) {}
   bool ok() const { return (bool)in_; }
   int line() const { return line_; }
 
@@ -39,6 +45,7 @@ class ListReader {
   bool read(std::vector<std::string>& items, int n) {
     items.clear();
     if (!next_line()) return false;
+    comma_open_ = true;   // a comma before the first value is a null value
     while ((int)items.size() < n) {
       std::string tok;
       if (!next_token(tok)) {
@@ -78,9 +85,18 @@ class ListReader {
     pos_ = 0;
     return true;
   }
+  // The next item of the READ: a value, or an empty string for a null value.
   bool next_token(std::string& tok) {
-    while (pos_ < buf_.size() && (std::isspace((unsigned char)buf_[pos_]) || buf_[pos_] == ','))
+    for (;;) {
+      while (pos_ < buf_.size() && std::isspace((unsigned char)buf_[pos_])) ++pos_;
+      if (pos_ >= buf_.size() || buf_[pos_] != ',') break;
       ++pos_;
+      if (comma_open_) {   // two separating commas: a null value
+        tok.clear();
+        return true;
+      }
+      comma_open_ = true;
+    }
     if (pos_ >= buf_.size()) return false;
     if (buf_[pos_] == '/') {
       slash_ = true;
@@ -92,9 +108,12 @@ class ListReader {
            buf_[pos_] != '/')
       ++pos_;
     tok = buf_.substr(b, pos_ - b);
+    comma_open_ = false;
     return true;
   }
-  std::ifstream in_;
+  std::unique_ptr<std::istream> own_;
+  std::istream& in_;
+  bool comma_open_ = false;   // a comma was read since the last value
   std::string buf_;
   size_t pos_ = 0;
   int line_ = 0;
@@ -177,16 +196,17 @@ int fmt2d_read_refl(const char* path, int* n, double* x, double* z) {
   std::string s;
   while (r.raw_line(s)) {
     if (s.find_first_not_of(" \t\r") == std::string::npos) continue;   // blank line
-    // two values from the line; a malformed line is skipped (:110-116)
-    for (char& c : s)
-      if (c == ',') c = ' ';
+    // every non-blank line counts against the limit before it is parsed
+    // (:105-109); a malformed line, or one with a null value, is skipped
+    // (:110-116)
+    if (xs.size() + 1 > 100000) return io_fail(FMT2D_ERR_MODEL, "refl file exceeds 100000 lines");
     std::istringstream ls(s);
-    std::string a, b;
+    ListReader lr(ls);
+    std::vector<std::string> it;
     double xv = 0, zv = 0;
-    if (!(ls >> a >> b) || !to_double(a, xv) || !to_double(b, zv)) continue;
+    if (!lr.read(it, 2) || !to_double(it[0], xv) || !to_double(it[1], zv)) continue;
     xs.push_back(xv);
     zs.push_back(zv);
-    if (xs.size() > 100000) return io_fail(FMT2D_ERR_MODEL, "refl file exceeds 100000 lines");
   }
   if (xs.empty()) return io_fail(FMT2D_ERR_MODEL, std::string("refl file has no valid data: ") + path);
   *n = (int)xs.size();

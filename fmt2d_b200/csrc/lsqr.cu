@@ -582,14 +582,24 @@ std::string Lsqr::solve(const LsqrParams& p, const double* residual, const doubl
   dm_.alloc((size_t)np_ * 8);
   if (!res_.p || !dms_.p || !gtg_.p || !mask_.p || !u_.p || !v_.p || !w_.p || !dm_.p)
     return "device allocation failed (LSQR vectors)";
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  if (nd_ && !residual) return "null residual";
+  // events and the iteration graph are released on every return path
+  struct Res {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~Res() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } r;
+  LCK(cudaEventCreate(&r.e0));
+  LCK(cudaEventCreate(&r.e1));
+  cudaEvent_t e0 = r.e0, e1 = r.e1;
   cudaEventRecord(e0, st_);
-  if (nd_) {
-    if (!residual) return "null residual";
-    LCK(cudaMemcpyAsync(res_.p, residual, (size_t)nd_ * 8, cudaMemcpyHostToDevice, st_));
-  }
+  if (nd_) LCK(cudaMemcpyAsync(res_.p, residual, (size_t)nd_ * 8, cudaMemcpyHostToDevice, st_));
   if (dm_sum) LCK(cudaMemcpyAsync(dms_.p, dm_sum, (size_t)np_ * 8, cudaMemcpyHostToDevice, st_));
   else LCK(cudaMemsetAsync(dms_.p, 0, (size_t)np_ * 8, st_));
   LsqrDev d = view();
@@ -614,15 +624,14 @@ std::string Lsqr::solve(const LsqrParams& p, const double* residual, const doubl
   launches += 4;
   LCK(cudaGetLastError());
   // the iteration loop: a graph of kIterPerGraph (adj, fwd) pairs
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
   LCK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < kIterPerGraph; ++k) {
     lsqr_launch_adj(d, grid_, st_);
     lsqr_launch_fwd(d, grid_, st_);
   }
-  LCK(cudaStreamEndCapture(st_, &graph));
-  LCK(cudaGraphInstantiate(&exec, graph, 0));
+  LCK(cudaStreamEndCapture(st_, &r.graph));
+  LCK(cudaGraphInstantiate(&r.exec, r.graph, 0));
+  cudaGraphExec_t exec = r.exec;
   const int max_graphs = p.max_iter / kIterPerGraph + 2;
   std::string err;
   for (int gi = 0; gi <= max_graphs; ++gi) {
@@ -638,10 +647,6 @@ std::string Lsqr::solve(const LsqrParams& p, const double* residual, const doubl
   LCK(cudaStreamSynchronize(st_));
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
   last_ms_ = ms;
   last_launches_ = launches;
   if (!err.empty()) return err;
@@ -679,23 +684,51 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 namespace {
 
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[256] = {};
+struct NoAllocAddr {
+  void* ctx = nullptr;    // CUcontext the address was looked up in
+  void* ptr = nullptr;
+};
+NoAllocAddr g_noalloc_addr[256];
+
+// CUcontext current on this thread (the driver call is reached through the
+// runtime's entry-point query, so the library need not link the driver).
+void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrent>(f);
+    looked = true;
+  }
+  void* c = nullptr;
+  if (fn) fn(&c);
+  return c;
+}
 
 // Device address of the scratch array on `device` (which must be current).
-// The first call on a device looks it up with cudaGetSymbolAddress: in host
-// code the array's name is only a host-side stand-in, so kernels must be
-// given this address.
+// It is looked up with cudaGetSymbolAddress on the first call in a CUDA
+// context of the device (in host code the array's name is only a host-side
+// stand-in, so kernels must be given this address) and again whenever the
+// device's context changed since (after cudaDeviceReset the module is loaded
+// anew and the array may sit elsewhere).
 std::string noalloc_scratch(int device, double** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (device < 0 || device >= 256) return "device ordinal out of range";
-  if (!g_noalloc_ptr[device]) {
+  void* ctx = current_context();
+  NoAllocAddr& a = g_noalloc_addr[device];
+  if (!a.ptr || ctx != a.ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e);
-    g_noalloc_ptr[device] = p;
+    a.ptr = p;
+    a.ctx = current_context();
   }
-  *out = static_cast<double*>(g_noalloc_ptr[device]);
+  *out = static_cast<double*>(a.ptr);
   return std::string();
 }
 

@@ -256,9 +256,14 @@ FMT2D_API int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params, const 
  * set by fmt2d_set_frechet.  The work vectors live in one fixed 32 MiB device
  * array that every GPU loading the library holds until exit; problems that
  * need more (about ndata + 6.125 nparm doubles) are rejected with
- * FMT2D_ERR_ARG.  The first call on a device looks up that array's address,
- * so make it before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race. */
+ * FMT2D_ERR_ARG.  The first call in a device's CUDA context looks up that
+ * array's address, so make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race.
+ * Ordering: the call runs on the context's own stream (fmt2d_stream), which
+ * is not ordered after the streams the caller wrote residual, gtg_diag and
+ * dm_sum on; make those writes complete first (synchronise, or make the
+ * stream fmt2d_stream returns wait on an event recorded after them).  dm and
+ * the scalars are final when the call returns. */
 FMT2D_API int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* params,
                                  const double* residual, const double* gtg_diag,
                                  const double* dm_sum, double* dm, int* iters, double* rnorm,

@@ -93,3 +93,35 @@ def test_errors(tmp_path):
     r.write_text("\nabc\n")
     with pytest.raises(N.Fmt2dError, match="no valid data"):
         io.read_refl(str(r))
+
+
+def test_null_values_are_not_shifted(tmp_path):
+    """Two commas with only blanks between them are a null value in
+    list-directed input (the variable stays unset), not a wider separator:
+    the values after it keep their positions, and the null item is reported
+    as unreadable."""
+    from fmt2d_b200 import _native as N
+    f = tmp_path / "null.smesh"
+    f.write_text("3 2 1.5 0.33\n0.0,, 2.0\n2.5 2.5 2.5\n0.0 1.0\n4 4 4\n5 5 5\n")
+    with pytest.raises(N.Fmt2dError, match="xpos"):
+        io.read_smesh(str(f))
+    r = tmp_path / "null.dat"
+    r.write_text("0.0 20.0\n1.0,,21.0\n2.0 , 22.0\n")
+    x, z = io.read_refl(str(r))
+    np.testing.assert_array_equal(x, [0.0, 2.0])
+    np.testing.assert_array_equal(z, [20.0, 22.0])
+
+
+def test_refl_line_limit_counts_every_nonblank_line(tmp_path):
+    """read_refl stops at 100000 data lines; a further non-blank line fails
+    the read even when it is malformed (read_tomo2d.f90:105-109 counts the
+    line before parsing it)."""
+    from fmt2d_b200 import _native as N
+    r = tmp_path / "long.dat"
+    body = "".join(f"{i * 0.01:.2f} 20.0\n" for i in range(100000))
+    r.write_text(body + "\n  \n")
+    x, _ = io.read_refl(str(r))
+    assert x.size == 100000
+    r.write_text(body + "not a line\n")
+    with pytest.raises(N.Fmt2dError, match="exceeds 100000"):
+        io.read_refl(str(r))
