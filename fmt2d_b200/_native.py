@@ -33,7 +33,20 @@ class LsqrParams(C.Structure):
 
 
 class Fmt2dError(RuntimeError):
-    pass
+    """A library call failed; `code` is its FMT2D_ERR_* status."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
+
+
+class Fmt2dNotConverged(Fmt2dError):
+    """fmt2d_forward returned FMT2D_ERR_CONVERGE: a time field did not reach
+    its fixed point (nodes still moving after the last check, or the step cap
+    reached)."""
+
+
+ERR_CONVERGE = -5
 
 
 def header_symbols() -> list[str]:
@@ -66,7 +79,7 @@ def lib():
     L.fmt2d_get_field.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_stats.argtypes = [V, C.c_void_p, C.c_int]
     L.fmt2d_stream.argtypes = [V, P(V)]
-    L.fmt2d_set_schedule.argtypes = [V, C.c_double, C.c_int]
+    L.fmt2d_set_schedule.argtypes = [V, C.c_double, C.c_int, C.c_longlong]
     L.fmt2d_read_smesh.argtypes = [C.c_char_p, P(C.c_int), P(C.c_int), P(C.c_double),
                                    P(C.c_double)] + [C.c_void_p] * 4
     L.fmt2d_read_refl.argtypes = [C.c_char_p, P(C.c_int), C.c_void_p, C.c_void_p]

@@ -110,7 +110,8 @@ class Fmt2d:
         if rc != 0:
             buf = C.create_string_buffer(512)
             self.L.fmt2d_last_error(self.h, buf, 512)
-            raise N.Fmt2dError(f"{what} failed ({rc}): {buf.value.decode()}")
+            cls = N.Fmt2dNotConverged if rc == N.ERR_CONVERGE else N.Fmt2dError
+            raise cls(f"{what} failed ({rc}): {buf.value.decode()}", rc)
 
     def upload(self, m: SmeshModel, iface_inv: int = 4):
         f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
@@ -317,13 +318,14 @@ class Fmt2d:
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
 
-    def set_schedule(self, window_cells: float = 0.5, max_passes: int = 6):
+    def set_schedule(self, window_cells: float = 0.5, max_passes: int = 6, max_steps: int = 0):
         """Eikonal solve schedule (fmt2d_set_schedule).  The time window bounds
         how far ahead of the settled times a node may be written; the default
         (0.5 cells) is the one the parity tests use.  max_passes bounds the
-        solve passes (each ends in a fixed-point check of every node)."""
-        self._check(self.L.fmt2d_set_schedule(self.h, float(window_cells), int(max_passes)),
-                    "fmt2d_set_schedule")
+        solve passes (each ends in a fixed-point check of every node),
+        max_steps the steps of one field's solve (0: the library default)."""
+        self._check(self.L.fmt2d_set_schedule(self.h, float(window_cells), int(max_passes),
+                                              int(max_steps)), "fmt2d_set_schedule")
         return self
 
     def stream(self) -> int:

@@ -389,13 +389,16 @@ int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
   return FMT2D_OK;
 }
 
-int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes) {
-  if (!ctx || !(window_cells > 0.0) || window_cells > 64.0 || max_passes < 1 || max_passes > 64)
+int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
+                       long long max_steps) {
+  if (!ctx || !(window_cells > 0.0) || window_cells > 64.0 || max_passes < 1 || max_passes > 64 ||
+      max_steps < 0)
     return FMT2D_ERR_ARG;
   int code = 0;
   if (!ctx->need_gpu(code)) return code;
   ctx->eng->window_cells = window_cells;
   ctx->eng->max_passes = max_passes;
+  ctx->eng->max_steps = max_steps > 0 ? max_steps : fmt2d::Engine::kDefaultMaxSteps;
   return FMT2D_OK;
 }
 

@@ -98,7 +98,10 @@ Engine::~Engine() {
 std::string Engine::upload(const Model& m) {
   cudaSetDevice(device_);
   m_ = m;
-  fields_.clear();
+  // the field stores stay allocated (a store grows when a region does);
+  // every field is unsolved until the next forward
+  for (auto& src : fields_)
+    for (FieldStore& f : src) f.solved = false;
   std::string e;
   for (int r = 1; r <= 6; ++r) {
     const Region& G = m.reg[r];
@@ -443,10 +446,9 @@ std::string Engine::get_field(int src, int tf, double* T, double* gx, double* gz
   const Region& G = m_.reg[kTf[tf].reg];
   const DevRegionStore& D = reg_[kTf[tf].reg];
   const int nn = G.nnode;
-  DevBuf out;
-  out.alloc((size_t)nn * 3 * sizeof(double));
-  if (!out.p) return "device allocation failed";
-  double* d = out.as<double>();
+  export_.alloc((size_t)nn * 3 * sizeof(double));
+  if (!export_.p) return "device allocation failed";
+  double* d = export_.as<double>();
   e64_export(F.T.as<double>(), F.Gout.as<double2>(), D.slot_of_node.as<int>(), nn, d, d + nn,
              d + 2 * (size_t)nn, stream_);
   ++stats_.launches;

@@ -79,7 +79,8 @@ class Engine {
   // the last forward failed because a field did not reach its fixed point
   bool not_converged() const { return not_converged_; }
   double window_cells = 0.5; // window step: this many cells at the region's largest velocity
-  long long max_steps = 4000000;  // safety cap on the steps of one field's solve
+  static constexpr long long kDefaultMaxSteps = 4000000;
+  long long max_steps = kDefaultMaxSteps;  // safety cap on the steps of one field's solve
   int max_passes = 6;             // solve passes (each followed by a check of every node)
   // device pointers of a solved field (FP64 time, double2 final gradient per slot)
   const double* field_t(int src, int tf) const { return fields_[src][tf].T.as<double>(); }
@@ -104,6 +105,7 @@ class Engine {
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
   DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_scratch_, d_which_, d_up_, d_step_, d_ctr_;
+  DevBuf export_;             // region-order copy of a field being read back
   DevBuf d_sTn_, d_sGn_, d_sfln_, d_spend_, d_slist_, d_sover_, d_sinq_, d_scnt_;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
       d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;

@@ -274,13 +274,15 @@ FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* Schedule of the eikonal solve (no reference counterpart; the reference's
  * heap has no schedule): the time window's step in cells at the region's
- * largest velocity (0 < window_cells <= 64, default 0.5) and the number of
+ * largest velocity (0 < window_cells <= 64, default 0.5), the number of
  * solve passes, each followed by a fixed-point check of every node
- * (1..64, default 6); a forward whose last check still finds nodes that
- * move returns FMT2D_ERR_CONVERGE.  The window bounds how far ahead of the
- * settled times a node may be written; the default is the one the parity
- * tests use. */
-FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes);
+ * (1..64, default 6), and the most steps one field's solve may take
+ * (0: the default, 4,000,000).  A forward whose last check still finds
+ * nodes that move, or in which a field reached the step cap, returns
+ * FMT2D_ERR_CONVERGE.  The window bounds how far ahead of the settled times
+ * a node may be written; the default is the one the parity tests use. */
+FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
+                                 long long max_steps);
 
 /* The CUDA stream (cudaStream_t) all work of the context is issued on, for
  * callers that record events around fmt2d_forward.  No reference counterpart. */

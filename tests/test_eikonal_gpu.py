@@ -60,3 +60,79 @@ def test_pg_401x121(oracle_lib):
         for tf in (1, 4, 5):
             emax, g99 = _compare(o, g, s, s, tf)
             assert emax <= T_TOL, f"src {s} tf{tf}: max |dT| = {emax * 1e3:.4f} ms"
+
+
+def _max_err(o, g, slot, src, tf):
+    To, _, _ = o.field(slot, tf)
+    Tg, _, _ = g.field(src, tf)
+    ro, rg = To < 1e19, Tg < 1e19
+    assert (ro == rg).all(), f"tf{tf}: reached sets differ ({(ro != rg).sum()} nodes)"
+    return float(np.abs(To[ro] - Tg[ro]).max()) if ro.any() else 0.0
+
+
+def test_benchmark_model_2001x401(oracle_lib):
+    """The benchmarked configuration itself (2001x401 at 0.1 km, Pg + PmP) on
+    four sources spread along the line, every stage against the FP64 heap
+    FMM: identical reached sets, <= 0.5 ms everywhere, and the gradient
+    statistics of the other tests."""
+    from fmt2d_b200.api import Fmt2d, phase_mask
+    m = synth.config(1)
+    o = oracle_lib.Oracle(m)
+    pick = [0, 9, 20, 29]
+    srcs = m.obs_x[pick]
+    g = Fmt2d(0).upload(m).forward(srcs, (1, 3))
+    st = g.stats()
+    assert st["capped"] == 0 and st["unsettled"] == 0
+    for s, sx in enumerate(srcs):
+        o.forward(s, float(sx), phase_mask((1, 3)))
+        for tf in (1, 4, 5):
+            emax, g99 = _compare(o, g, s, s, tf)
+            assert emax <= T_TOL, f"src {pick[s]} tf{tf}: max |dT| = {emax * 1e3:.4f} ms"
+            assert g99 <= 0.02, f"src {pick[s]} tf{tf}: 99% gradient error {g99:.4f}"
+
+
+def test_largest_model_4001x601(oracle_lib):
+    """The 4001x601 model (0.1 km, sediment + Moho) on two sources with Pg,
+    PsedP and PmP (five stage fields each) against the oracle."""
+    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
+    m = synth.config(4)
+    o = oracle_lib.Oracle(m)
+    srcs = m.obs_x[[10, 70]]
+    mask = phase_mask((1, 2, 3))
+    g = Fmt2d(0).upload(m).forward(srcs, (1, 2, 3))
+    for s, sx in enumerate(srcs):
+        o.forward(s, float(sx), mask)
+        for tf in fields_of(mask):
+            emax = _max_err(o, g, s, s, tf)
+            assert emax <= T_TOL, f"src {s} tf{tf}: max |dT| = {emax * 1e3:.4f} ms"
+
+
+def test_forward_is_deterministic():
+    """The solve's phases (evaluate from committed values, commit, spread)
+    make its result independent of thread timing: two forwards of the same
+    sources give bit-identical times and gradients in every stage field."""
+    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
+    m = synth.config(1)
+    srcs = m.obs_x[[3, 17]]
+    g = Fmt2d(0).upload(m)
+    runs = []
+    for _ in range(2):
+        g.forward(srcs, (1, 3))
+        runs.append([g.field(s, tf) for s in range(srcs.size) for tf in fields_of(phase_mask((1, 3)))])
+    for a, b in zip(*runs):
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.int64), y.view(np.int64))
+
+
+def test_step_cap_is_reported():
+    """A solve stopped by the step cap is an error (FMT2D_ERR_CONVERGE), never
+    a silently unconverged field; the default schedule then solves again."""
+    from fmt2d_b200 import _native as N
+    from fmt2d_b200.api import Fmt2d
+    m = synth.small_model()
+    g = Fmt2d(0).upload(m).set_schedule(max_steps=5)
+    with pytest.raises(N.Fmt2dNotConverged):
+        g.forward(m.obs_x, (1, 3))
+    assert g.stats()["capped"] > 0
+    g.set_schedule().forward(m.obs_x, (1, 3))
+    assert g.stats()["capped"] == 0 and g.stats()["unsettled"] == 0
