@@ -17,10 +17,11 @@
 // One thread block owns a field for the whole solve: the lists, the
 // "listed" bitset and the window live in shared memory, steps are separated
 // by block barriers instead of kernel launches, and the field's front stays
-// in the SM's L1.  A step has three phases separated by barriers: evaluate
-// (reads committed state only, stages new values per slot), commit, spread.
-// Evaluations therefore never see a value of the same step, so the result
-// does not depend on thread timing: a forward is bit-identical run to run.
+// in the SM's L1.  A step has four phases separated by barriers: evaluate
+// (reads committed state only, stages new values per slot), arbitrate,
+// commit, spread.  Evaluations never see a value of the same step, so the
+// result does not depend on thread timing: a forward is bit-identical run to
+// run.
 //
 // Arithmetic is FP64 with the reference's expression order; this file is
 // compiled with --fmad=false so candidate times are bit-identical to the
@@ -45,7 +46,9 @@ constexpr unsigned kCCap = 2048;          // commit entries held in shared memor
 constexpr int kTileRows = 8;              // a tile: 8 slot rows x 32 slot columns (one bitset word per row)
 constexpr int kTilesMax = 12288;          // tiles per field (tile minima live in shared memory)
 constexpr size_t kSmemMax = 227 * 1024;   // dynamic shared memory of the solve block
-constexpr unsigned kSpreadBit = 0x80000000u;
+constexpr unsigned kSpreadBit = 0x80000000u;   // commit entry: the node moved
+constexpr unsigned kLostBit = 0x40000000u;     // commit entry: lost arbitration, listed again
+constexpr unsigned kSlotMask = 0x3fffffffu;
 constexpr unsigned long long kNone = ULLONG_MAX;
 
 struct SolveShared {
@@ -178,11 +181,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       else cov[p - kCCap] = e;
       if (nv.spread) {
         sh.changed[par] = 1;
-        ++n_write;
+        F.claim[s] = dbits(nv.T);
       }
     }
     __syncthreads();
-    // commit (the old time stays in Tn for the spread threshold)
+    // arbitrate: a moving node commits only if no node that reads it (the
+    // nodes it reads are among them) moves to a smaller (time, slot) in the
+    // same step; the others are listed again.  Of two nodes that feed each
+    // other the earlier goes first, as the heap accepts them, so a pair that
+    // hands a time back and forth (a zero-increment update) cannot swap
+    // values forever.
     const unsigned nc = sh.nc[par];
     if (tid == 0) {
       sh.cnt[cur] = 0u;
@@ -190,7 +198,33 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       sh.changed[par ^ 1] = 0;
     }
     for (unsigned j = tid; j < nc; j += kSolveThreads) {
-      const unsigned s = (j < kCCap ? scl[j] : cov[j - kCCap]) & ~kSpreadBit;
+      const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
+      if (!(e & kSpreadBit)) continue;
+      const int s = (int)(e & kSlotMask);
+      const unsigned long long ks = F.claim[s];
+      int t[16];
+      const int k = spread_targets(F, s, t);
+      bool lose = false;
+      for (int q = 0; q < k; ++q) {
+        const unsigned long long kt = F.claim[t[q]];
+        lose = lose || kt < ks || (kt == ks && t[q] < s);
+      }
+      if (lose) {
+        if (j < kCCap) scl[j] = e | kLostBit;
+        else cov[j - kCCap] = e | kLostBit;
+      }
+    }
+    __syncthreads();
+    // commit the winners (the old time stays in Tn for the spread threshold)
+    for (unsigned j = tid; j < nc; j += kSolveThreads) {
+      const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
+      const unsigned s = e & kSlotMask;
+      if (e & kSpreadBit) F.claim[s] = kNone;
+      if (e & kLostBit) {
+        push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
+        continue;
+      }
+      if (e & kSpreadBit) ++n_write;
       const double old = F.T[s];
       F.T[s] = F.Tn[s];
       F.Tn[s] = old;
@@ -204,8 +238,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     // computed from the old value, which is dropped
     for (unsigned j = tid; j < nc; j += kSolveThreads) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
-      if (!(e & kSpreadBit)) continue;
-      const int s = (int)(e & ~kSpreadBit);
+      if (!(e & kSpreadBit) || (e & kLostBit)) continue;
+      const int s = (int)(e & kSlotMask);
       const double thr = fmin(F.Tn[s], F.T[s]);
       int t[16];
       const int k = spread_targets(F, s, t);
@@ -353,6 +387,7 @@ __global__ void k_fill(Fld64* fields, int nf) {
     F.seed[i] = make_double4(kHugeD, 0.0, 0.0, 0.0);
     F.fl[i] = 0;
     F.pend[i] = -1.0;
+    F.claim[i] = ULLONG_MAX;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) F.frozen_slot = -1;
 }

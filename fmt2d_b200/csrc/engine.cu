@@ -270,7 +270,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     total += D.nslots;
     max_slots = std::max(max_slots, D.nslots);
   }
-  if (total >= 0x7fffffffull) return "batch too large for 31-bit slot ids";
+  if (max_slots >= (1ull << 30)) return "region too large for the eikonal solver (2^30 slots)";
   // solver scratch of the batch, per slot: staged time, gradient and flags,
   // pending time, start list, list and commit overflow, listed bitset
   const size_t words = (total + 31 * (size_t)nf + 31) / 32 + (size_t)nf;
@@ -278,12 +278,13 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   d_sGn_.alloc(total * sizeof(double2));
   d_sfln_.alloc(total);
   d_spend_.alloc(total * sizeof(double));
+  d_sclaim_.alloc(total * sizeof(unsigned long long));
   d_slist_.alloc(total * sizeof(unsigned));
   d_sover_.alloc(3 * total * sizeof(unsigned));
   d_sinq_.alloc(2 * words * sizeof(unsigned));
   d_scnt_.alloc((size_t)nf * 4 * sizeof(unsigned));
   d_ctr_.alloc(kCtrN * sizeof(unsigned long long));
-  if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_slist_.p || !d_sover_.p ||
+  if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_sclaim_.p || !d_slist_.p || !d_sover_.p ||
       !d_sinq_.p || !d_scnt_.p || !d_ctr_.p)
     return "device allocation failed for the solver scratch";
   size_t base = 0, wbase = 0;
@@ -296,6 +297,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     hf[i].Gn = d_sGn_.as<double2>() + base;
     hf[i].fln = d_sfln_.as<uint8_t>() + base;
     hf[i].pend = d_spend_.as<double>() + base;
+    hf[i].claim = d_sclaim_.as<unsigned long long>() + base;
     hf[i].list_in = d_slist_.as<unsigned>() + base;
     hf[i].over = d_sover_.as<unsigned>() + 3 * base;
     hf[i].inq = d_sinq_.as<unsigned>() + wbase;

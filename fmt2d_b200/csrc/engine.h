@@ -106,7 +106,7 @@ class Engine {
   std::vector<double> src_x_, src_z_;
   DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_scratch_, d_which_, d_up_, d_step_, d_ctr_;
   DevBuf export_;             // region-order copy of a field being read back
-  DevBuf d_sTn_, d_sGn_, d_sfln_, d_spend_, d_slist_, d_sover_, d_sinq_, d_scnt_;
+  DevBuf d_sTn_, d_sGn_, d_sfln_, d_spend_, d_sclaim_, d_slist_, d_sover_, d_sinq_, d_scnt_;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
       d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
   int npick_ = -1, rows_ = 0;
