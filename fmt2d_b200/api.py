@@ -210,7 +210,8 @@ class Fmt2d:
         return T, gx, gz
 
     STATS = ("steps", "batches", "passes", "passed", "solve_ms", "launches", "nodes",
-             "evals", "steps_all", "capped", "writes", "unsettled")
+             "evals", "steps_all", "capped", "writes", "unsettled", "cyc_eval", "cyc_arb",
+             "cyc_commit", "cyc_spread", "cyc_release", "cut_evals")
 
     def stats(self) -> dict:
         """Counters of the last forward (fmt2d_stats)."""

@@ -254,7 +254,9 @@ int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
   const double v[FMT2D_N_STATS] = {
       (double)s.rounds,    (double)s.batches, (double)s.final_passes, (double)s.passed,
       s.round_ms,          (double)s.launches, (double)s.nodes,       (double)s.evals,
-      (double)s.steps_sum, (double)s.capped,  (double)s.writes,       (double)s.unsettled};
+      (double)s.steps_sum, (double)s.capped,  (double)s.writes,       (double)s.unsettled,
+      s.cycles[0],         s.cycles[1],       s.cycles[2],            s.cycles[3],
+      s.cycles[4],         (double)s.cut_evals};
   for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
   return FMT2D_OK;
 }

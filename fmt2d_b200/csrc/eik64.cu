@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   __syncthreads();
   double W = F.clock[0];
   const double wstep = F.clock[1];
-  unsigned long long n_eval = 0, n_write = 0, n_rel = 0;
+  unsigned long long n_eval = 0, n_write = 0, n_rel = 0, n_cut = 0;
+  unsigned long long cyc[5] = {0, 0, 0, 0, 0};   // thread 0: cycles per phase
+  long long c0 = clock64();
   int cur = 0, rp = 0;
   long long it = 0;
   for (;; ++it) {
@@ -160,6 +162,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       atomicAnd(bits + (s >> 5), ~(1u << (s & 31)));
       const NewV nv = evaluate(F, (int)s);
       ++n_eval;
+      n_cut += (FMT_RO(F.code + s) & kFullyRegular) ? 0 : 1;
       if (!nv.write) {
         F.pend[s] = -1.0;
         continue;
@@ -185,6 +188,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       }
     }
     __syncthreads();
+    if (tid == 0) {
+      const long long c1 = clock64();
+      cyc[0] += (unsigned long long)(c1 - c0);
+      c0 = c1;
+    }
     // arbitrate: a moving node commits only if no node that reads it (the
     // nodes it reads are among them) moves to a smaller (time, slot) in the
     // same step; the others are listed again.  Of two nodes that feed each
@@ -215,6 +223,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       }
     }
     __syncthreads();
+    if (tid == 0) {
+      const long long c1 = clock64();
+      cyc[1] += (unsigned long long)(c1 - c0);
+      c0 = c1;
+    }
     // commit the winners (the old time stays in Tn for the spread threshold)
     for (unsigned j = tid; j < nc; j += kSolveThreads) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
@@ -232,6 +245,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       F.fl[s] = F.fln[s];
     }
     __syncthreads();
+    if (tid == 0) {
+      const long long c1 = clock64();
+      cyc[2] += (unsigned long long)(c1 - c0);
+      c0 = c1;
+    }
     // spread: every candidate of a node u that involves node v is at or above
     // v's time, so a change of v from a to b can only move nodes at or above
     // min(a, b); those below are not listed unless they wait with a time
@@ -250,6 +268,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       }
     }
     __syncthreads();
+    if (tid == 0) {
+      const long long c1 = clock64();
+      cyc[3] += (unsigned long long)(c1 - c0);
+      c0 = c1;
+    }
     // the window moves on after a step that changed nothing inside it (or
     // listed nothing); the tiles it reaches release their due nodes, and when
     // none is due it jumps to the earliest waiting time
@@ -309,6 +332,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
         if (g == kNone) break;
         W = fmax(W, __longlong_as_double((long long)g));
       }
+      if (tid == 0) {
+        const long long c1 = clock64();
+        cyc[4] += (unsigned long long)(c1 - c0);
+        c0 = c1;
+      }
     }
     cur = nxt;
   }
@@ -317,8 +345,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     n_eval += __shfl_xor_sync(0xffffffffu, n_eval, o);
     n_write += __shfl_xor_sync(0xffffffffu, n_write, o);
     n_rel += __shfl_xor_sync(0xffffffffu, n_rel, o);
+    n_cut += __shfl_xor_sync(0xffffffffu, n_cut, o);
   }
   if (lane == 0 && ctr) {
+    atomicAdd(ctr + kCtrCut, n_cut);
     atomicAdd(ctr + kCtrEval, n_eval);
     atomicAdd(ctr + kCtrWrite, n_write);
     atomicAdd(ctr + kCtrPass, n_rel);
@@ -331,6 +361,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     F.cnt[3] = (unsigned)(it < 0xffffffffll ? it : 0xffffffffll);
     if (sh.err) F.cnt[2] = 1u;
     if (ctr) {
+      for (int k = 0; k < 5; ++k) atomicAdd(ctr + kCtrCycEval + k, cyc[k]);
       atomicAdd(ctr + kCtrSteps, (unsigned long long)it);
       atomicMax(ctr + kCtrMaxSteps, (unsigned long long)it);
     }

@@ -75,7 +75,13 @@ struct Seed64 {
 // Solver counters summed over a batch: evaluations, committed writes that
 // changed a node, waiting nodes released by the window, steps (summed over
 // fields), largest step count of one field.
-enum { kCtrEval = 0, kCtrWrite, kCtrPass, kCtrSteps, kCtrMaxSteps, kCtrN };
+// Also: SM cycles of the solve's phases (evaluate, arbitrate, commit, spread,
+// window release; summed over fields) and evaluations of nodes next to an
+// interface (cut-cell updates).
+enum {
+  kCtrEval = 0, kCtrWrite, kCtrPass, kCtrSteps, kCtrMaxSteps,
+  kCtrCycEval, kCtrCycArb, kCtrCycCommit, kCtrCycSpread, kCtrCycRelease, kCtrCut, kCtrN
+};
 
 void e64_fill(Fld64* f, int nf, size_t max_slots, cudaStream_t st);
 void e64_init_source(Fld64* f, const double* sx, const double* sz, int nf, cudaStream_t st);

@@ -412,6 +412,8 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     stats_.passed += c[kCtrPass];
     stats_.rounds += (long long)c[kCtrMaxSteps];
     stats_.steps_sum += c[kCtrSteps];
+    for (int k = 0; k < 5; ++k) stats_.cycles[k] += (double)c[kCtrCycEval + k];
+    stats_.cut_evals += c[kCtrCut];
   }
   if (bad) {
     stats_.unsettled += bad;

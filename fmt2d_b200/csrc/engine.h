@@ -53,6 +53,8 @@ struct SolveStats {
   unsigned long long capped = 0;      // fields that reached the step cap
   long long launches = 0;     // kernels launched since the last forward began
   long long nodes = 0;        // region nodes of the time fields solved
+  double cycles[5] = {0, 0, 0, 0, 0};   // SM cycles of the solve phases, summed over fields
+  unsigned long long cut_evals = 0;     // evaluations of nodes next to an interface
 };
 
 class Engine {
