@@ -41,6 +41,7 @@ using namespace ev;
 // ---------------------------------------------------------------- field solve
 constexpr int kSolveThreads = 256;
 constexpr int kSolveWarps = kSolveThreads / 32;
+constexpr int kHalfWarps = kSolveThreads / 16;
 constexpr unsigned kLCap = 4096;          // entries of each list held in shared memory
 constexpr unsigned kCCap = 2048;          // commit entries held in shared memory
 constexpr int kTileRows = 8;              // a tile: 8 slot rows x 32 slot columns (one bitset word per row)
@@ -103,6 +104,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   extern __shared__ __align__(16) unsigned char dsm_raw[];
   __shared__ SolveShared sh;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int hw = tid >> 4, hl = tid & 15;                 // half-warp, its lane
+  const unsigned hmask = 0xffffu << (16 * (hw & 1));
   if (tid == 0) {
     sh.F = fields[blockIdx.x];
     sh.cnt[0] = sh.cnt[1] = 0u;
@@ -205,19 +208,20 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       sh.nc[par ^ 1] = 0u;
       sh.changed[par ^ 1] = 0;
     }
-    for (unsigned j = tid; j < nc; j += kSolveThreads) {
+    // (a half-warp per moved node, a lane per node that reads it)
+    for (unsigned j = hw; j < nc; j += kHalfWarps) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
       if (!(e & kSpreadBit)) continue;
       const int s = (int)(e & kSlotMask);
       const unsigned long long ks = F.claim[s];
-      int t[16];
-      const int k = spread_targets(F, s, t);
+      const int t = spread_target_at(F, s, hl);
       bool lose = false;
-      for (int q = 0; q < k; ++q) {
-        const unsigned long long kt = F.claim[t[q]];
-        lose = lose || kt < ks || (kt == ks && t[q] < s);
+      if (t >= 0) {
+        const unsigned long long kt = F.claim[t];
+        lose = kt < ks || (kt == ks && t < s);
       }
-      if (lose) {
+      const unsigned lost = __ballot_sync(hmask, lose) & hmask;
+      if (hl == 0 && lost) {
         if (j < kCCap) scl[j] = e | kLostBit;
         else cov[j - kCCap] = e | kLostBit;
       }
@@ -254,18 +258,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     // v's time, so a change of v from a to b can only move nodes at or above
     // min(a, b); those below are not listed unless they wait with a time
     // computed from the old value, which is dropped
-    for (unsigned j = tid; j < nc; j += kSolveThreads) {
+    for (unsigned j = hw; j < nc; j += kHalfWarps) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
       if (!(e & kSpreadBit) || (e & kLostBit)) continue;
       const int s = (int)(e & kSlotMask);
+      const int t = spread_target_at(F, s, hl);
+      if (t < 0) continue;
       const double thr = fmin(F.Tn[s], F.T[s]);
-      int t[16];
-      const int k = spread_targets(F, s, t);
-      for (int q = 0; q < k; ++q) {
-        const bool waiting = F.pend[t[q]] >= 0.0;
-        F.pend[t[q]] = -1.0;
-        if (waiting || !(F.T[t[q]] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t[q]);
-      }
+      const bool waiting = F.pend[t] >= 0.0;
+      F.pend[t] = -1.0;
+      if (waiting || !(F.T[t] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t);
     }
     __syncthreads();
     if (tid == 0) {
@@ -294,28 +296,34 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
         for (unsigned k = warp; k < nr; k += kSolveWarps) {
           const int t = ready[k];
           const int r0 = (t / tcols) * kTileRows, c0 = (t % tcols) * 32;
+          // lane l takes column c0 + l of the tile's rows; the rows' loads
+          // are issued together
+          unsigned word[kTileRows];
+          double pd[kTileRows];
+#pragma unroll
+          for (int rr = 0; rr < kTileRows; ++rr)
+            word[rr] = r0 + rr < F.H + 2 ? wbits[(unsigned)((r0 + rr) * F.pitch + c0) >> 5] : 0u;
+#pragma unroll
+          for (int rr = 0; rr < kTileRows; ++rr)
+            pd[rr] = (word[rr] >> lane) & 1u ? F.pend[(r0 + rr) * F.pitch + c0 + lane] : 0.0;
           unsigned long long m = kNone;
+#pragma unroll
           for (int rr = 0; rr < kTileRows; ++rr) {
-            const int r = r0 + rr;
-            if (r >= F.H + 2) break;
-            const unsigned w = (unsigned)(r * F.pitch + c0) >> 5;
-            const unsigned word = wbits[w];
+            const bool set = (word[rr] >> lane) & 1u;
             bool clear = false;
-            if (word & (1u << lane)) {
-              const unsigned s = (unsigned)(r * F.pitch + c0 + lane);
-              const double pd = F.pend[s];
-              if (pd < 0.0) {
+            if (set) {
+              if (pd[rr] < 0.0) {
                 clear = true;                 // listed since (an input changed)
-              } else if (pd <= W) {
+              } else if (pd[rr] <= W) {
                 clear = true;
-                push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
+                push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)((r0 + rr) * F.pitch + c0 + lane));
                 ++n_rel;
               } else {
-                m = min(m, dbits(pd));
+                m = min(m, dbits(pd[rr]));
               }
             }
             const unsigned cm = __ballot_sync(0xffffffffu, clear);
-            if (lane == 0 && cm) wbits[w] = word & ~cm;
+            if (lane == 0 && cm) wbits[(unsigned)((r0 + rr) * F.pitch + c0) >> 5] = word[rr] & ~cm;
           }
 #pragma unroll
           for (int o = 16; o; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));

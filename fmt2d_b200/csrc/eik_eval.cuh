@@ -657,45 +657,48 @@ FMT_HD void fit_grad(const Fld64& F, int slot, double& dtdx, double& dtdz) {
 // Final gradients: the winning candidate's, suspect nodes refitted
 
 // Nodes whose candidates read node `slot` (the nodes a change of it can
-// move): for a grid node its second neighbours along the axes, its 3x3 block
-// and the interface nodes of the cut cells it is a corner of; for an
-// interface node the corners of its cut cell and the node of the other
-// interface row in the same column.  Writes at most 16 slots to t and
-// returns their number.
-FMT_HD inline int spread_targets(const Fld64& F, int slot, int* t) {
+// move), by fixed position q = 0..15: for a grid node its second neighbours
+// along the axes and its 3x3 block (q < 12) and the interface nodes of the
+// cut cells it is a corner of (q = 12..15); for an interface node the corners
+// of its cut cell (q < 4) and the node of the other interface row in the
+// same column (q = 4).  Returns the target's slot, or -1 where position q
+// holds no node.
+FMT_HD inline int spread_target_at(const Fld64& F, int slot, int q) {
   const int row = slot / F.pitch, c = slot - row * F.pitch;
-  int n = 0;
   if (row < F.H) {
-    const int r = row;
-    const int dr[12] = {-2, 2, 0, 0, -1, -1, -1, 0, 0, 1, 1, 1};
-    const int dc[12] = {0, 0, -2, 2, -1, 0, 1, -1, 1, -1, 0, 1};
-    for (int k = 0; k < 12; ++k) {
-      const int rr = r + dr[k], cc = c + dc[k];
-      if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) continue;
+    if (q < 12) {
+      const int dr = q < 2 ? (q == 0 ? -2 : 2) : (q < 4 ? 0 : (q < 7 ? -1 : (q < 9 ? 0 : 1)));
+      const int dc = q < 2 ? 0 : (q < 4 ? (q == 2 ? -2 : 2)
+                                        : (q < 7 ? q - 5 : (q < 9 ? (q == 7 ? -1 : 1) : q - 10)));
+      const int rr = row + dr, cc = c + dc;
+      if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) return -1;
       const int s = rr * F.pitch + cc;
-      if (FMT_RO(F.code + s) & kInRegion) t[n++] = s;
+      return (FMT_RO(F.code + s) & kInRegion) ? s : -1;
     }
-    const int ar = F.z_lo + r;
-    for (int k = 0; k < 4; ++k) {
-      const int side = k >> 1, kc = c - 1 + (k & 1);
-      if (kc < 0 || kc >= F.nx) continue;
-      const int izc = FMT_RO(F.izc + side * F.pitch + kc);
-      if (izc >= 0 && (izc == ar || izc + 1 == ar)) t[n++] = (F.H + side) * F.pitch + kc;
-    }
-    return n;
+    const int k = q - 12, side = k >> 1, kc = c - 1 + (k & 1);
+    if (kc < 0 || kc >= F.nx) return -1;
+    const int izc = FMT_RO(F.izc + side * F.pitch + kc), ar = F.z_lo + row;
+    return (izc >= 0 && (izc == ar || izc + 1 == ar)) ? (F.H + side) * F.pitch + kc : -1;
   }
   const int side = row - F.H;
+  if (q == 4) return (F.H + (side ^ 1)) * F.pitch + c;
+  if (q > 4) return -1;
   const int izc = FMT_RO(F.izc + side * F.pitch + c);
-  if (izc >= 0) {
-    const int br = izc - F.z_lo;
-    for (int k = 0; k < 4; ++k) {
-      const int rr = br + (k & 1), cc = c + (k >> 1);
-      if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) continue;
-      const int s = rr * F.pitch + cc;
-      if (FMT_RO(F.code + s) & kInRegion) t[n++] = s;
-    }
+  if (izc < 0) return -1;
+  const int rr = izc - F.z_lo + (q & 1), cc = c + (q >> 1);
+  if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) return -1;
+  const int s = rr * F.pitch + cc;
+  return (FMT_RO(F.code + s) & kInRegion) ? s : -1;
+}
+
+// The same targets as a list: writes at most 16 slots to t, returns their
+// number.
+FMT_HD inline int spread_targets(const Fld64& F, int slot, int* t) {
+  int n = 0;
+  for (int q = 0; q < 16; ++q) {
+    const int s = spread_target_at(F, slot, q);
+    if (s >= 0) t[n++] = s;
   }
-  t[n++] = (F.H + (side ^ 1)) * F.pitch + c;
   return n;
 }
 
