@@ -211,7 +211,7 @@ class Fmt2d:
 
     STATS = ("steps", "batches", "passes", "passed", "solve_ms", "launches", "nodes",
              "evals", "steps_all", "capped", "writes", "unsettled", "cyc_eval", "cyc_arb",
-             "cyc_commit", "cyc_spread", "cyc_release", "cut_evals")
+             "cyc_eval_cut", "cyc_spread", "cyc_release", "cut_evals", "cut_steps")
 
     def stats(self) -> dict:
         """Counters of the last forward (fmt2d_stats)."""

@@ -256,7 +256,7 @@ int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
       s.round_ms,          (double)s.launches, (double)s.nodes,       (double)s.evals,
       (double)s.steps_sum, (double)s.capped,  (double)s.writes,       (double)s.unsettled,
       s.cycles[0],         s.cycles[1],       s.cycles[2],            s.cycles[3],
-      s.cycles[4],         (double)s.cut_evals};
+      s.cycles[4],         (double)s.cut_evals, (double)s.cut_steps};
   for (int i = 0; i < n && i < FMT2D_N_STATS; ++i) values[i] = v[i];
   return FMT2D_OK;
 }

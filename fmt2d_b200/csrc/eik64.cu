@@ -57,6 +57,7 @@ struct SolveShared {
   unsigned cnt[2];                 // list lengths
   unsigned nc[2];                  // commit list length, by step parity
   int changed[2];                  // a committed write moved a node, by step parity
+  int cutstep[2];                  // the step evaluated a node next to an interface
   unsigned nready[2];              // tiles to release, by release parity
   unsigned long long gmin[2];      // earliest waiting time (bits of a positive double)
   int err;
@@ -111,6 +112,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     sh.cnt[0] = sh.cnt[1] = 0u;
     sh.nc[0] = sh.nc[1] = 0u;
     sh.changed[0] = sh.changed[1] = 0;
+    sh.cutstep[0] = sh.cutstep[1] = 0;
     sh.nready[0] = sh.nready[1] = 0u;
     sh.gmin[0] = sh.gmin[1] = kNone;
     sh.err = 0;
@@ -148,6 +150,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const double wstep = F.clock[1];
   unsigned long long n_eval = 0, n_write = 0, n_rel = 0, n_cut = 0;
   unsigned long long cyc[5] = {0, 0, 0, 0, 0};   // thread 0: cycles per phase
+  unsigned long long steps_cut = 0;
   long long c0 = clock64();
   int cur = 0, rp = 0;
   long long it = 0;
@@ -165,7 +168,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       atomicAnd(bits + (s >> 5), ~(1u << (s & 31)));
       const NewV nv = evaluate(F, (int)s);
       ++n_eval;
-      n_cut += (FMT_RO(F.code + s) & kFullyRegular) ? 0 : 1;
+      if (!(FMT_RO(F.code + s) & kFullyRegular)) {
+        ++n_cut;
+        sh.cutstep[par] = 1;
+      }
       if (!nv.write) {
         F.pend[s] = -1.0;
         continue;
@@ -194,6 +200,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     if (tid == 0) {
       const long long c1 = clock64();
       cyc[0] += (unsigned long long)(c1 - c0);
+      if (sh.cutstep[par]) {
+        cyc[2] += (unsigned long long)(c1 - c0);
+        ++steps_cut;
+      }
       c0 = c1;
     }
     // arbitrate: a moving node commits only if no node that reads it (the
@@ -207,23 +217,38 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       sh.cnt[cur] = 0u;
       sh.nc[par ^ 1] = 0u;
       sh.changed[par ^ 1] = 0;
+      sh.cutstep[par ^ 1] = 0;
     }
-    // (a half-warp per moved node, a lane per node that reads it)
+    // (a half-warp per moved node, a lane per node that reads it); a winner
+    // commits at once (nothing reads committed times in this phase; the old
+    // time stays in Tn for the spread threshold)
     for (unsigned j = hw; j < nc; j += kHalfWarps) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
-      if (!(e & kSpreadBit)) continue;
       const int s = (int)(e & kSlotMask);
-      const unsigned long long ks = F.claim[s];
-      const int t = spread_target_at(F, s, hl);
       bool lose = false;
-      if (t >= 0) {
-        const unsigned long long kt = F.claim[t];
-        lose = kt < ks || (kt == ks && t < s);
+      if (e & kSpreadBit) {
+        const unsigned long long ks = F.claim[s];
+        const int t = spread_target_at(F, s, hl);
+        bool l = false;
+        if (t >= 0) {
+          const unsigned long long kt = F.claim[t];
+          l = kt < ks || (kt == ks && t < s);
+        }
+        lose = (__ballot_sync(hmask, l) & hmask) != 0u;
       }
-      const unsigned lost = __ballot_sync(hmask, lose) & hmask;
-      if (hl == 0 && lost) {
-        if (j < kCCap) scl[j] = e | kLostBit;
-        else cov[j - kCCap] = e | kLostBit;
+      if (hl == 0) {
+        if (lose) {
+          if (j < kCCap) scl[j] = e | kLostBit;
+          else cov[j - kCCap] = e | kLostBit;
+          push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)s);
+        } else {
+          if (e & kSpreadBit) ++n_write;
+          const double old = F.T[s];
+          F.T[s] = F.Tn[s];
+          F.Tn[s] = old;
+          F.G[s] = F.Gn[s];
+          F.fl[s] = F.fln[s];
+        }
       }
     }
     __syncthreads();
@@ -232,36 +257,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       cyc[1] += (unsigned long long)(c1 - c0);
       c0 = c1;
     }
-    // commit the winners (the old time stays in Tn for the spread threshold)
-    for (unsigned j = tid; j < nc; j += kSolveThreads) {
-      const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
-      const unsigned s = e & kSlotMask;
-      if (e & kSpreadBit) F.claim[s] = kNone;
-      if (e & kLostBit) {
-        push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], s);
-        continue;
-      }
-      if (e & kSpreadBit) ++n_write;
-      const double old = F.T[s];
-      F.T[s] = F.Tn[s];
-      F.Tn[s] = old;
-      F.G[s] = F.Gn[s];
-      F.fl[s] = F.fln[s];
-    }
-    __syncthreads();
-    if (tid == 0) {
-      const long long c1 = clock64();
-      cyc[2] += (unsigned long long)(c1 - c0);
-      c0 = c1;
-    }
     // spread: every candidate of a node u that involves node v is at or above
     // v's time, so a change of v from a to b can only move nodes at or above
     // min(a, b); those below are not listed unless they wait with a time
     // computed from the old value, which is dropped
     for (unsigned j = hw; j < nc; j += kHalfWarps) {
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
-      if (!(e & kSpreadBit) || (e & kLostBit)) continue;
+      if (!(e & kSpreadBit)) continue;
       const int s = (int)(e & kSlotMask);
+      if (hl == 0) F.claim[s] = kNone;   // every reader of the claims is done
+      if (e & kLostBit) continue;
       const int t = spread_target_at(F, s, hl);
       if (t < 0) continue;
       const double thr = fmin(F.Tn[s], F.T[s]);
@@ -370,6 +375,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     if (sh.err) F.cnt[2] = 1u;
     if (ctr) {
       for (int k = 0; k < 5; ++k) atomicAdd(ctr + kCtrCycEval + k, cyc[k]);
+      atomicAdd(ctr + kCtrStepsCut, steps_cut);
       atomicAdd(ctr + kCtrSteps, (unsigned long long)it);
       atomicMax(ctr + kCtrMaxSteps, (unsigned long long)it);
     }

@@ -75,12 +75,14 @@ struct Seed64 {
 // Solver counters summed over a batch: evaluations, committed writes that
 // changed a node, waiting nodes released by the window, steps (summed over
 // fields), largest step count of one field.
-// Also: SM cycles of the solve's phases (evaluate, arbitrate, commit, spread,
-// window release; summed over fields) and evaluations of nodes next to an
-// interface (cut-cell updates).
+// Also: SM cycles of the solve's phases summed over fields (evaluate,
+// arbitrate and commit, the evaluate phases of steps that evaluated a node
+// next to an interface, spread, window release), evaluations of nodes next
+// to an interface (cut-cell updates) and the steps that had one.
 enum {
   kCtrEval = 0, kCtrWrite, kCtrPass, kCtrSteps, kCtrMaxSteps,
-  kCtrCycEval, kCtrCycArb, kCtrCycCommit, kCtrCycSpread, kCtrCycRelease, kCtrCut, kCtrN
+  kCtrCycEval, kCtrCycArb, kCtrCycEvalCut, kCtrCycSpread, kCtrCycRelease, kCtrCut, kCtrStepsCut,
+  kCtrN
 };
 
 void e64_fill(Fld64* f, int nf, size_t max_slots, cudaStream_t st);

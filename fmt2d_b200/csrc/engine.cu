@@ -414,6 +414,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     stats_.steps_sum += c[kCtrSteps];
     for (int k = 0; k < 5; ++k) stats_.cycles[k] += (double)c[kCtrCycEval + k];
     stats_.cut_evals += c[kCtrCut];
+    stats_.cut_steps += c[kCtrStepsCut];
   }
   if (bad) {
     stats_.unsettled += bad;

@@ -55,6 +55,7 @@ struct SolveStats {
   long long nodes = 0;        // region nodes of the time fields solved
   double cycles[5] = {0, 0, 0, 0, 0};   // SM cycles of the solve phases, summed over fields
   unsigned long long cut_evals = 0;     // evaluations of nodes next to an interface
+  unsigned long long cut_steps = 0;     // steps that evaluated such a node
 };
 
 class Engine {

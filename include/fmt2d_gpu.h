@@ -188,10 +188,12 @@ FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double
  * fields, [9] fields that reached the step cap, [10] node writes that changed
  * a node, [11] nodes the last fixed-point check found still moving (nonzero
  * only when fmt2d_forward returned FMT2D_ERR_CONVERGE), [12..16] SM cycles of
- * the solve's phases summed over fields (evaluate, arbitrate, commit,
- * spread, window release), [17] evaluations of nodes next to an interface.
+ * the solve's phases summed over fields (evaluate, arbitrate and commit, the
+ * evaluate phases of steps with a node next to an interface, spread, window
+ * release), [17] evaluations of nodes next to an interface, [18] steps that
+ * evaluated one.
  * Writes min(n, FMT2D_N_STATS) values.  No reference counterpart (diagnostics). */
-#define FMT2D_N_STATS 18
+#define FMT2D_N_STATS 19
 FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
 
 /* Ray backtrace and Frechet rows of npick picks on the fields of the last
