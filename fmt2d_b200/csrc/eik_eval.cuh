@@ -73,15 +73,26 @@ FMT_HD inline double xg(const Fld64& F, int col) { return F.x0 + (double)col * F
 FMT_HD inline double zg(const Fld64& F, int brow) { return (double)(F.z_lo + brow) * F.dx; }
 
 // ---------------------------------------------------------------- candidates
+// A candidate carries its event and the operands of its gradient; the
+// gradient itself (divisions and a square root) is formed for the winner
+// only, by the same expressions the reference evaluates when a candidate
+// lowers the node.
+enum : uint8_t { kGradNone = 0, kGradReg, kGradRay, kGradPlane, kGradGiven };
+
 struct Cand {
-  double t, trig, gx, gz;
+  double t, trig;
+  double g0, g1, g2, g3, g4, g5;   // gradient operands, by kind (grad_of)
   int ord;
+  uint8_t kind;
+  bool gxi, gzi;                   // regular: the x / z neighbour took part
   bool sus, copy;
 };
 
 FMT_HD inline Cand no_cand() {
   Cand c;
-  c.t = kHugeD; c.trig = kHugeD; c.gx = 0.0; c.gz = 0.0; c.ord = 0x7fffffff;
+  c.t = kHugeD; c.trig = kHugeD; c.ord = 0x7fffffff;
+  c.g0 = c.g1 = c.g2 = c.g3 = c.g4 = c.g5 = 0.0;
+  c.kind = kGradNone; c.gxi = c.gzi = false;
   c.sus = false; c.copy = false;
   return c;
 }
@@ -90,11 +101,41 @@ FMT_HD inline bool earlier(double trig, int ord, const Cand& b) {
   return trig < b.trig || (trig == b.trig && ord < b.ord);
 }
 
-FMT_HD inline void take(Cand& best, double t, double trig, int ord, double gx,
-                                     double gz, bool sus, bool copy) {
-  if (t < best.t || (t == best.t && earlier(trig, ord, best))) {
-    best.t = t; best.trig = trig; best.ord = ord; best.gx = gx; best.gz = gz;
-    best.sus = sus; best.copy = copy;
+// Keep c (its t, trig and ord set) if it beats best.
+FMT_HD inline void take(Cand& best, const Cand& c) {
+  if (c.t < best.t || (c.t == best.t && earlier(c.trig, c.ord, best))) best = c;
+}
+
+// The gradient a winning candidate writes: regular_update2d's one-sided first
+// or second-order differences (:766-782), time_from_1_node2d's straight ray
+// (:823-826), time_from_2_nodes2d's plane-wave normal (:921-940) or a member's
+// gradient handed over.
+FMT_HD inline void grad_of(const Cand& w, double& gx, double& gz) {
+  gx = 0.0;
+  gz = 0.0;
+  switch (w.kind) {
+    case kGradReg:
+      if (w.gxi)
+        gx = (w.g1 == 0.0) ? (w.t - w.g0) / w.g2 : 0.5 * (3.0 * w.t - 4.0 * w.g0 + w.g1) / w.g2;
+      if (w.gzi)
+        gz = (w.g4 == 0.0) ? (w.t - w.g3) / w.g5 : 0.5 * (3.0 * w.t - 4.0 * w.g3 + w.g4) / w.g5;
+      break;
+    case kGradRay:
+      gx = w.g0 / (w.g2 * w.g3);
+      gz = w.g1 / (w.g2 * w.g3);
+      break;
+    case kGradPlane: {
+      const double wl = sqrt(w.g0 * w.g0 + w.g1 * w.g1);
+      gx = w.g0 / (wl * w.g2);
+      gz = w.g1 / (wl * w.g2);
+      break;
+    }
+    case kGradGiven:
+      gx = w.g0;
+      gz = w.g1;
+      break;
+    default:
+      break;
   }
 }
 
@@ -121,21 +162,29 @@ FMT_HD void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
     s1[k] = b1[k] ? rn * F.pitch + cn : 0;
     s2[k] = b2[k] ? r2 * F.pitch + c2 : 0;
   }
+  // codes, times, velocities and gradients are loaded in one round: a slot
+  // inside the band but outside the region holds huge_time (never written),
+  // so its time is read safely and discarded below
   uint32_t k1[4], k2[4];
+  double t1[4], t2[4], v1[4], v2[4];
+  double2 g1[4], g2[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     k1[k] = b1[k] ? FMT_RO(F.code + s1[k]) : 0u;
     k2[k] = b2[k] ? FMT_RO(F.code + s2[k]) : 0u;
-  }
-  double t1[4], t2[4], v1[4], v2[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    b1[k] = b1[k] && (k1[k] & kInRegion);
-    b2[k] = b2[k] && (k2[k] & kInRegion);
     t1[k] = b1[k] ? ldT(F, s1[k]) : kHugeD;
     v1[k] = b1[k] ? FMT_RO(F.vel + s1[k]) : 0.0;
     t2[k] = b2[k] ? ldT(F, s2[k]) : kHugeD;
     v2[k] = b2[k] ? FMT_RO(F.vel + s2[k]) : 0.0;
+    g1[k] = b2[k] ? ldG(F, s1[k]) : make_double2(0.0, 0.0);
+    g2[k] = b2[k] ? ldG(F, s2[k]) : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    b1[k] = b1[k] && (k1[k] & kInRegion);
+    b2[k] = b2[k] && (k2[k] & kInRegion);
+    if (!b1[k]) t1[k] = kHugeD;
+    if (!b2[k]) t2[k] = kHugeD;
   }
   bool need[4];
 #pragma unroll
@@ -158,12 +207,6 @@ FMT_HD void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
     if (!(v1[k] * v2[k] > kTinyD)) continue;
     need[k] = true;
   }
-  double2 g1[4], g2[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    g1[k] = need[k] ? ldG(F, s1[k]) : make_double2(0.0, 0.0);
-    g2[k] = need[k] ? ldG(F, s2[k]) : make_double2(0.0, 0.0);
-  }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (need[k] && g1[k].x * g2[k].x + g1[k].y * g2[k].y >= 0.71 / (v1[k] * v2[k])) {
@@ -173,9 +216,9 @@ FMT_HD void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
   }
 }
 
-// regular_update2d (:605-790) for one or two accepted neighbours.
-FMT_HD bool reg_cand(const RNb* p, const RNb* q, double& t1, double& gx, double& gz,
-                         bool& sus) {
+// regular_update2d (:605-790) for one or two accepted neighbours: the
+// candidate time, its suspect flag and its gradient operands.
+FMT_HD bool reg_cand(const RNb* p, const RNb* q, Cand& o) {
   double a = 0.0, b = 0.0, c = 0.0, t2x = 0.0, t2z = 0.0, tx = 0.0, tz = 0.0, tmax = 0.0;
   double dpx = 1.0, dpz = 1.0;
   bool xi = false, zi = false;
@@ -223,13 +266,15 @@ FMT_HD bool reg_cand(const RNb* p, const RNb* q, double& t1, double& gx, double&
     if (0.5 * sqrt(fabs(det)) / fabs(a) < 1.0e20) det = 0.0;
     else return false;
   }
-  t1 = 0.5 * (-b + sqrt(det)) / a;
-  t1 = fmax(t1, tmax);
-  gx = 0.0;
-  gz = 0.0;
-  if (xi) gx = (t2x == 0.0) ? (t1 - tx) / dpx : 0.5 * (3.0 * t1 - 4.0 * tx + t2x) / dpx;
-  if (zi) gz = (t2z == 0.0) ? (t1 - tz) / dpz : 0.5 * (3.0 * t1 - 4.0 * tz + t2z) / dpz;
-  sus = !(xi && zi);
+  const double t1 = 0.5 * (-b + sqrt(det)) / a;
+  o.t = fmax(t1, tmax);
+  o.kind = kGradReg;
+  o.gxi = xi;
+  o.gzi = zi;
+  o.g0 = tx; o.g1 = t2x; o.g2 = dpx;
+  o.g3 = tz; o.g4 = t2z; o.g5 = dpz;
+  o.sus = !(xi && zi);
+  o.copy = false;
   return true;
 }
 
@@ -237,18 +282,29 @@ FMT_HD bool reg_cand(const RNb* p, const RNb* q, double& t1, double& gx, double&
 // update of the earlier neighbour (triggered while the other was not yet
 // accepted) and the two-sided update (triggered by the later one).
 FMT_HD void quadrant(const RNb& X, const RNb& Z, int ord, Cand& best) {
-  double t, gx, gz;
-  bool sus;
+  Cand c;
+  c.ord = ord;
   if (X.ok && Z.ok) {
     const bool xlow = X.T <= Z.T;
     const RNb& lo = xlow ? X : Z;
-    if (lo.single_ok && reg_cand(&lo, nullptr, t, gx, gz, sus))
-      take(best, t, lo.T, ord, gx, gz, sus, false);
-    if (reg_cand(&X, &Z, t, gx, gz, sus)) take(best, t, fmax(X.T, Z.T), ord, gx, gz, sus, false);
+    if (lo.single_ok && reg_cand(&lo, nullptr, c)) {
+      c.trig = lo.T;
+      take(best, c);
+    }
+    if (reg_cand(&X, &Z, c)) {
+      c.trig = fmax(X.T, Z.T);
+      take(best, c);
+    }
   } else if (X.ok) {
-    if (X.single_ok && reg_cand(&X, nullptr, t, gx, gz, sus)) take(best, t, X.T, ord, gx, gz, sus, false);
+    if (X.single_ok && reg_cand(&X, nullptr, c)) {
+      c.trig = X.T;
+      take(best, c);
+    }
   } else if (Z.ok) {
-    if (Z.single_ok && reg_cand(&Z, nullptr, t, gx, gz, sus)) take(best, t, Z.T, ord, gx, gz, sus, false);
+    if (Z.single_ok && reg_cand(&Z, nullptr, c)) {
+      c.trig = Z.T;
+      take(best, c);
+    }
   }
 }
 
@@ -268,10 +324,22 @@ struct CutAcc {
   int rord;
 };
 
-FMT_HD inline void offer(CutAcc& A, double t, double trig, int ord, double gx,
-                                      double gz, bool copy) {
-  take(A.best, t, trig, ord, gx, gz, false, copy);
+FMT_HD inline void offer(CutAcc& A, Cand& c, double t, double trig, int ord, bool copy) {
+  c.t = t;
+  c.trig = trig;
+  c.ord = ord;
+  c.sus = false;
+  c.copy = copy;
+  take(A.best, c);
   if (trig < A.rtrig || (trig == A.rtrig && ord < A.rord)) A.pre_min = fmin(A.pre_min, t);
+}
+
+// Gradient operands of a member's gradient handed over, of a straight ray
+// from a member, of a plane front.
+FMT_HD inline void given(Cand& c, double gx, double gz) {
+  c.kind = kGradGiven;
+  c.g0 = gx;
+  c.g1 = gz;
 }
 
 // time_from_1_node2d (:793-829).  A member closer than 0.01*tolerance hands
@@ -282,13 +350,22 @@ FMT_HD void from_1(const Mem& a, double xu, double zu, double vu, double tol, do
                        int ord, CutAcc& A) {
   const double dxu = xu - a.x, dzu = zu - a.z;
   const double dist = sqrt(dxu * dxu + dzu * dzu);
+  Cand c;
   if (dist < 0.01 * tol) {
-    if (!a.copied) offer(A, a.T, trig, ord, a.gx, a.gz, true);
+    if (!a.copied) {
+      given(c, a.gx, a.gz);
+      offer(A, c, a.T, trig, ord, true);
+    }
     return;
   }
   const double tt = dist / (0.5 * (vu + a.v));
   const double at = a.T + tt;
-  offer(A, at, trig, ord, dxu / (dist * vu), dzu / (dist * vu), false);
+  c.kind = kGradRay;
+  c.g0 = dxu;
+  c.g1 = dzu;
+  c.g2 = dist;
+  c.g3 = vu;
+  offer(A, c, at, trig, ord, false);
 }
 
 // time_from_2_nodes2d (:832-946): planar front through the trigger n1 and an
@@ -298,12 +375,19 @@ FMT_HD void from_2(const Mem& n1, const Mem& n2, double xu, double zu, double vu
   const double trig = n1.T;
   const double r1x = n1.x - xu, r1z = n1.z - zu;
   const double r2x = n2.x - xu, r2z = n2.z - zu;
+  Cand c;
   if (sqrt(r1x * r1x + r1z * r1z) < 0.01 * tol) {
-    if (!n1.copied) offer(A, n1.T, trig, ord, n1.gx, n1.gz, true);
+    if (!n1.copied) {
+      given(c, n1.gx, n1.gz);
+      offer(A, c, n1.T, trig, ord, true);
+    }
     return;
   }
   if (sqrt(r2x * r2x + r2z * r2z) < 0.01 * tol) {
-    if (!n2.copied) offer(A, n2.T, trig, ord, n2.gx, n2.gz, true);
+    if (!n2.copied) {
+      given(c, n2.gx, n2.gz);
+      offer(A, c, n2.T, trig, ord, true);
+    }
     return;
   }
   const double ex = n2.x - n1.x, ez = n2.z - n1.z;
@@ -341,8 +425,11 @@ FMT_HD void from_2(const Mem& n1, const Mem& n2, double xu, double zu, double vu
     if (wx * m1x + wz * m1z <= 0.0 && wx * m2x + wz * m2z <= 0.0) {
       const double at = n1.T - (wx * r1x + wz * r1z) / (0.5 * (vu + n1.v));
       if (at >= n1.T) {
-        const double wl = sqrt(wx * wx + wz * wz);
-        offer(A, at, trig, ord, wx / (wl * n1.v), wz / (wl * n1.v), false);
+        c.kind = kGradPlane;
+        c.g0 = wx;
+        c.g1 = wz;
+        c.g2 = n1.v;
+        offer(A, c, at, trig, ord, false);
       }
     }
   }
@@ -431,7 +518,9 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
   NewV o;
   o.write = false;
   o.spread = false;
-  double T = w.t < kReachD ? w.t : kHugeD, gx = w.gx, gz = w.gz;
+  double gx, gz;
+  grad_of(w, gx, gz);
+  double T = w.t < kReachD ? w.t : kHugeD;
   bool su = sus, cp = w.copy;
   const uint8_t fl = ldF(F, s);
   if (fl & kFlSeed) {
