@@ -319,12 +319,13 @@ class Fmt2d:
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
 
-    def set_schedule(self, window_cells: float = 0.5, max_passes: int = 6, max_steps: int = 0):
-        """Eikonal solve schedule (fmt2d_set_schedule).  The time window bounds
-        how far ahead of the settled times a node may be written; the default
-        (0.5 cells) is the one the parity tests use.  max_passes bounds the
-        solve passes (each ends in a fixed-point check of every node),
-        max_steps the steps of one field's solve (0: the library default)."""
+    def set_schedule(self, window_cells: float = 0.0, max_passes: int = 6, max_steps: int = 0):
+        """Eikonal solve schedule (fmt2d_set_schedule).  window_cells > 0 holds
+        new times beyond a window of that many cells (at the region's largest
+        velocity) until the times below it settle; 0 (the default) sets no
+        window.  max_passes bounds the solve passes (each ends in a fixed-point
+        check of every node), max_steps the steps of one field's solve (0: the
+        library default)."""
         self._check(self.L.fmt2d_set_schedule(self.h, float(window_cells), int(max_passes),
                                               int(max_steps)), "fmt2d_set_schedule")
         return self

@@ -393,7 +393,7 @@ int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches) {
 
 int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
                        long long max_steps) {
-  if (!ctx || !(window_cells > 0.0) || window_cells > 64.0 || max_passes < 1 || max_passes > 64 ||
+  if (!ctx || !(window_cells >= 0.0) || window_cells > 1.0e6 || max_passes < 1 || max_passes > 64 ||
       max_steps < 0)
     return FMT2D_ERR_ARG;
   int code = 0;

@@ -26,6 +26,7 @@ struct Fld64 {
   const double* ifz = nullptr;      // 2*pitch: interface node z (top, bottom)
   int H = 0, pitch = 0, z_lo = 0, nx = 0, nz = 0;
   double x0 = 0, dx = 0, tol = 0;
+  double eps = 0.0;                 // change threshold (0: solve to the last bit)
   double* T = nullptr;              // per slot
   double2* G = nullptr;             // per slot: gradient of the winning candidate
   double2* Gout = nullptr;          // per slot: final gradient (suspect nodes refitted)

@@ -547,6 +547,12 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
   o.T = T; o.gx = gx; o.gz = gz; o.sus = su; o.copy = cp;
   o.spread = gchg;
   o.write = gchg || su != ((fl & kFlSusp) != 0);
+  // with a change threshold, a move smaller than it (time in s, gradient in
+  // s/km) is stored but re-lists nobody: the fixed point is then solved to
+  // within the threshold instead of to the last bit
+  if (gchg && F.eps > 0.0 && cp == ((fl & kFlCopy) != 0) && curT < kReachD && T < kReachD &&
+      fabs(T - curT) <= F.eps && fabs(gx - cg.x) <= F.eps && fabs(gz - cg.y) <= F.eps)
+    o.spread = false;
   return o;
 }
 

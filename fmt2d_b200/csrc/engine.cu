@@ -308,7 +308,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     base += D.nslots;
     wbase += (D.nslots + 31) / 32;
     up[i] = kTf[tf].water_up;
-    wstep[i] = window_cells * m_.dx / D.vmax;
+    wstep[i] = window_cells > 0.0 ? window_cells * m_.dx / D.vmax : kHugeD;
     if (tf == 5) hw.push_back(i);
   }
   std::string e;

@@ -81,7 +81,7 @@ class Engine {
   const SolveStats& stats() const { return stats_; }
   // the last forward failed because a field did not reach its fixed point
   bool not_converged() const { return not_converged_; }
-  double window_cells = 0.5; // window step: this many cells at the region's largest velocity
+  double window_cells = 0.0; // window step in cells at the region's largest velocity (0: no window)
   static constexpr long long kDefaultMaxSteps = 4000000;
   long long max_steps = kDefaultMaxSteps;  // safety cap on the steps of one field's solve
   int max_passes = 6;             // solve passes (each followed by a check of every node)

@@ -278,13 +278,17 @@ FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* Schedule of the eikonal solve (no reference counterpart; the reference's
  * heap has no schedule): the time window's step in cells at the region's
- * largest velocity (0 < window_cells <= 64, default 0.5), the number of
- * solve passes, each followed by a fixed-point check of every node
- * (1..64, default 6), and the most steps one field's solve may take
- * (0: the default, 4,000,000).  A forward whose last check still finds
+ * largest velocity (0 <= window_cells <= 1e6; 0, the default, sets no
+ * window), the number of solve passes, each followed by a fixed-point check
+ * of every node (1..64, default 6), and the most steps one field's solve may
+ * take (0: the default, 4,000,000).  A forward whose last check still finds
  * nodes that move, or in which a field reached the step cap, returns
- * FMT2D_ERR_CONVERGE.  The window bounds how far ahead of the settled times
- * a node may be written; the default is the one the parity tests use. */
+ * FMT2D_ERR_CONVERGE.  A window holds back every new time beyond it until
+ * the times below it have settled (nodes settle in time slices); without one
+ * a step commits, among nodes that read each other, the smallest new time
+ * first, which already orders dependent nodes as the heap does.  Both
+ * schedules reproduce the heap's times in the parity tests; the window
+ * takes more steps. */
 FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
                                  long long max_steps);
 

@@ -82,7 +82,8 @@ def test_argument_checks_of_later_entry_points(native):
     assert L.fmt2d_set_frechet(g.h, 1, 5, rp, i1, d1, 3) == -1
     assert L.fmt2d_set_frechet(g.h, 1, 5, rp, i1, d1, 1) == -3
     # fmt2d_set_schedule: ranges
-    assert L.fmt2d_set_schedule(g.h, 0.0, 6, 0) == -1
+    assert L.fmt2d_set_schedule(g.h, -1.0, 6, 0) == -1
+    assert L.fmt2d_set_schedule(g.h, 2.0e6, 6, 0) == -1
     assert L.fmt2d_set_schedule(g.h, 0.5, 0, 0) == -1
     assert L.fmt2d_set_schedule(g.h, 0.5, 65, 0) == -1
     assert L.fmt2d_set_schedule(g.h, 0.5, 6, -1) == -1

@@ -34,13 +34,16 @@ def _compare(o, g, slot, src, tf):
     return err.max() if err.size else 0.0, np.quantile(gerr, 0.99) if gerr.size else 0.0
 
 
+@pytest.mark.parametrize("window", [0.0, 0.5])
 @pytest.mark.parametrize("phases", [(1,), (3,), (1, 2, 3, 4, 5)])
-def test_small_model_all_fields(oracle_lib, phases):
+def test_small_model_all_fields(oracle_lib, phases, window):
+    """Every stage field of the five phases on the small model, with the
+    default schedule (no window) and with a half-cell time window."""
     from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
     m = synth.small_model()
     o = oracle_lib.Oracle(m)
     mask = phase_mask(phases)
-    g = Fmt2d(0).upload(m).forward(m.obs_x, phases)
+    g = Fmt2d(0).upload(m).set_schedule(window_cells=window).forward(m.obs_x, phases)
     for s, sx in enumerate(m.obs_x):
         o.forward(s, sx, mask)
         for tf in fields_of(mask):
