@@ -20,9 +20,27 @@ extern const TfInfo kTf[13];
 // phase -> time fields it needs (bit tf)
 unsigned phase_fields(int phase_mask);
 
+// Owning device buffer (move-only: a copy would free the memory twice).
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      free_();
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   void alloc(size_t n);
   void free_();
   ~DevBuf() { free_(); }

@@ -139,3 +139,21 @@ def test_step_cap_is_reported():
     assert g.stats()["capped"] > 0
     g.set_schedule().forward(m.obs_x, (1, 3))
     assert g.stats()["capped"] == 0 and g.stats()["unsettled"] == 0
+
+
+def test_more_sources_after_fewer():
+    """A context keeps its field stores between forwards; a forward with more
+    sources than the last one grows them without losing the device memory of
+    the stores it moves (same fields as a fresh context)."""
+    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
+    m = synth.small_model()
+    g = Fmt2d(0).upload(m)
+    g.forward(m.obs_x[:1], (1, 3))
+    g.forward(m.obs_x, (1, 3))
+    g.upload(m).forward(m.obs_x, (1, 3))
+    fresh = Fmt2d(0).upload(m).forward(m.obs_x, (1, 3))
+    for s in range(m.obs_x.size):
+        for tf in fields_of(phase_mask((1, 3))):
+            a, b = g.field(s, tf), fresh.field(s, tf)
+            for x, y in zip(a, b):
+                assert np.array_equal(x.view(np.int64), y.view(np.int64))
