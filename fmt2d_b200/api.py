@@ -322,8 +322,9 @@ class Fmt2d:
     def set_schedule(self, window_cells: float = 0.0, max_passes: int = 6, max_steps: int = 0):
         """Eikonal solve schedule (fmt2d_set_schedule).  window_cells > 0 holds
         new times beyond a window of that many cells (at the region's largest
-        velocity) until the times below it settle; 0 (the default) sets no
-        window.  max_passes bounds the solve passes (each ends in a fixed-point
+        velocity) until the times below it settle; 0 (the default) sets none
+        for stages that start from the point source and 32 cells for stages
+        seeded along an interface.  max_passes bounds the solve passes (each ends in a fixed-point
         check of every node), max_steps the steps of one field's solve (0: the
         library default)."""
         self._check(self.L.fmt2d_set_schedule(self.h, float(window_cells), int(max_passes),

@@ -132,11 +132,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   const bool local_bits = nbw <= (unsigned)smem_bits;
   unsigned* bits = local_bits ? sbits : F.inq;
   unsigned* wbits = local_bits ? sbits + smem_bits : F.wait;
+  unsigned* mbits = local_bits ? sbits + 2 * smem_bits : F.moving;
   unsigned* ov[2] = {F.over, F.over + ns};
   unsigned* cov = F.over + 2 * (size_t)ns;
   for (unsigned w = tid; w < nbw; w += kSolveThreads) {
     bits[w] = 0u;
     wbits[w] = 0u;
+    mbits[w] = 0u;
   }
   for (int t = tid; t < ntiles; t += kSolveThreads) tmin[t] = kNone;
   __syncthreads();
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       if (nv.spread) {
         sh.changed[par] = 1;
         F.claim[s] = dbits(nv.T);
+        atomicOr(mbits + (s >> 5), 1u << (s & 31));
       }
     }
     __syncthreads();
@@ -227,11 +230,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       const int s = (int)(e & kSlotMask);
       bool lose = false;
       if (e & kSpreadBit) {
-        const unsigned long long ks = F.claim[s];
-        const int t = spread_target_at(F, s, hl);
+        // only neighbours that move this step hold a claim (moving bitset)
+        const int t = neighbour_slot(F, s, hl);
         bool l = false;
-        if (t >= 0) {
-          const unsigned long long kt = F.claim[t];
+        if (t >= 0 && ((mbits[t >> 5] >> (t & 31)) & 1u)) {
+          const unsigned long long ks = F.claim[s], kt = F.claim[t];
           l = kt < ks || (kt == ks && t < s);
         }
         lose = (__ballot_sync(hmask, l) & hmask) != 0u;
@@ -265,13 +268,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       const unsigned e = j < kCCap ? scl[j] : cov[j - kCCap];
       if (!(e & kSpreadBit)) continue;
       const int s = (int)(e & kSlotMask);
-      if (hl == 0) F.claim[s] = kNone;   // every reader of the claims is done
+      if (hl == 0) atomicAnd(mbits + (s >> 5), ~(1u << (s & 31)));   // readers are done
       if (e & kLostBit) continue;
       const int t = spread_target_at(F, s, hl);
       if (t < 0) continue;
       const double thr = fmin(F.Tn[s], F.T[s]);
-      const bool waiting = F.pend[t] >= 0.0;
-      F.pend[t] = -1.0;
+      // a waiting target (its bit may be stale) drops the time it waits with
+      const bool waiting = (wbits[t >> 5] >> (t & 31)) & 1u;
+      if (waiting) F.pend[t] = -1.0;
       if (waiting || !(F.T[t] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t);
     }
     __syncthreads();
@@ -679,11 +683,11 @@ static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* t
                        (2 * (size_t)kLCap + kCCap) * sizeof(unsigned) +
                        (size_t)cap * sizeof(unsigned short);
   const size_t nbw = (max_slots + 31) / 32;
-  const size_t room = fixed + 1024 < kSmemMax ? (kSmemMax - fixed - 1024) / (2 * sizeof(unsigned)) : 0;
-  const size_t words = nbw <= room ? nbw : 0;   // both bitsets of every field fit, or none
+  const size_t room = fixed + 1024 < kSmemMax ? (kSmemMax - fixed - 1024) / (3 * sizeof(unsigned)) : 0;
+  const size_t words = nbw <= room ? nbw : 0;   // the three bitsets of every field fit, or none
   *smem_bits = (int)words;
   *tiles_cap = cap;
-  return fixed + 2 * words * sizeof(unsigned);
+  return fixed + 3 * words * sizeof(unsigned);
 }
 int e64_tiles(const Fld64& f) { return tiles_of(f); }
 int e64_tiles_max() { return kTilesMax; }

@@ -44,6 +44,7 @@ struct Fld64 {
   unsigned* over = nullptr;         // 3*nslots: list overflow (two lists) and commit overflow
   unsigned* inq = nullptr;          // bitset over slots: listed (when not in shared memory)
   unsigned* wait = nullptr;         // bitset over slots: waiting (when not in shared memory)
+  unsigned* moving = nullptr;       // bitset over slots: moving this step (when not in shared memory)
   unsigned* cnt = nullptr;          // [0] list_in length, [1] unsettled nodes found by a check,
                                     // [2] error (1: step cap), [3] steps of the last solve
 #if defined(__CUDACC__)

@@ -786,6 +786,33 @@ FMT_HD inline int spread_target_at(const Fld64& F, int slot, int q) {
   return (FMT_RO(F.code + s) & kInRegion) ? s : -1;
 }
 
+// Position q of the same neighbourhood without looking at the region: the
+// slot, or -1 outside the band (a superset of spread_target_at's nodes).
+FMT_HD inline int neighbour_slot(const Fld64& F, int slot, int q) {
+  const int row = slot / F.pitch, c = slot - row * F.pitch;
+  if (row < F.H) {
+    if (q < 12) {
+      const int dr = q < 2 ? (q == 0 ? -2 : 2) : (q < 4 ? 0 : (q < 7 ? -1 : (q < 9 ? 0 : 1)));
+      const int dc = q < 2 ? 0 : (q < 4 ? (q == 2 ? -2 : 2)
+                                        : (q < 7 ? q - 5 : (q < 9 ? (q == 7 ? -1 : 1) : q - 10)));
+      const int rr = row + dr, cc = c + dc;
+      if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) return -1;
+      return rr * F.pitch + cc;
+    }
+    const int k = q - 12, kc = c - 1 + (k & 1);
+    if (kc < 0 || kc >= F.nx) return -1;
+    return (F.H + (k >> 1)) * F.pitch + kc;
+  }
+  const int side = row - F.H;
+  if (q == 4) return (F.H + (side ^ 1)) * F.pitch + c;
+  if (q > 4) return -1;
+  const int izc = FMT_RO(F.izc + side * F.pitch + c);
+  if (izc < 0) return -1;
+  const int rr = izc - F.z_lo + (q & 1), cc = c + (q >> 1);
+  if (rr < 0 || rr >= F.H || cc < 0 || cc >= F.nx) return -1;
+  return rr * F.pitch + cc;
+}
+
 // The same targets as a list: writes at most 16 slots to t, returns their
 // number.
 FMT_HD inline int spread_targets(const Fld64& F, int slot, int* t) {

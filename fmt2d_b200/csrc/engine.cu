@@ -281,7 +281,7 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   d_sclaim_.alloc(total * sizeof(unsigned long long));
   d_slist_.alloc(total * sizeof(unsigned));
   d_sover_.alloc(3 * total * sizeof(unsigned));
-  d_sinq_.alloc(2 * words * sizeof(unsigned));
+  d_sinq_.alloc(3 * words * sizeof(unsigned));
   d_scnt_.alloc((size_t)nf * 4 * sizeof(unsigned));
   d_ctr_.alloc(kCtrN * sizeof(unsigned long long));
   if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_sclaim_.p || !d_slist_.p || !d_sover_.p ||
@@ -302,13 +302,20 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     hf[i].over = d_sover_.as<unsigned>() + 3 * base;
     hf[i].inq = d_sinq_.as<unsigned>() + wbase;
     hf[i].wait = d_sinq_.as<unsigned>() + words + wbase;
+    hf[i].moving = d_sinq_.as<unsigned>() + 2 * words + wbase;
     if (e64_tiles(hf[i]) > e64_tiles_max()) return "region too large for the eikonal solver";
     max_tiles = std::max(max_tiles, e64_tiles(hf[i]));
     hf[i].cnt = d_scnt_.as<unsigned>() + 4 * (size_t)i;
     base += D.nslots;
     wbase += (D.nslots + 31) / 32;
     up[i] = kTf[tf].water_up;
-    wstep[i] = window_cells > 0.0 ? window_cells * m_.dx / D.vmax : kHugeD;
+    // the schedule's window, or by default none for a point source and
+    // kIfaceWindowCells for a stage seeded along an interface (its seeds span
+    // the whole line at once; without a window far nodes take early times
+    // that many later updates revise)
+    const double wc = window_cells > 0.0 ? window_cells
+                      : (kTf[tf].level == 0 ? 0.0 : kIfaceWindowCells);
+    wstep[i] = wc > 0.0 ? wc * m_.dx / D.vmax : kHugeD;
     if (tf == 5) hw.push_back(i);
   }
   std::string e;

@@ -99,7 +99,10 @@ class Engine {
   const SolveStats& stats() const { return stats_; }
   // the last forward failed because a field did not reach its fixed point
   bool not_converged() const { return not_converged_; }
-  double window_cells = 0.0; // window step in cells at the region's largest velocity (0: no window)
+  // window step in cells at the region's largest velocity; 0: none for point
+  // sources, kIfaceWindowCells for stages seeded along an interface
+  double window_cells = 0.0;
+  static constexpr double kIfaceWindowCells = 32.0;
   static constexpr long long kDefaultMaxSteps = 4000000;
   long long max_steps = kDefaultMaxSteps;  // safety cap on the steps of one field's solve
   int max_passes = 6;             // solve passes (each followed by a check of every node)

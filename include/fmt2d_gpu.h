@@ -278,8 +278,10 @@ FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 
 /* Schedule of the eikonal solve (no reference counterpart; the reference's
  * heap has no schedule): the time window's step in cells at the region's
- * largest velocity (0 <= window_cells <= 1e6; 0, the default, sets no
- * window), the number of solve passes, each followed by a fixed-point check
+ * largest velocity for every stage (0 < window_cells <= 1e6), or 0, the
+ * default: no window for a stage that starts from the point source and 32
+ * cells for a stage seeded along an interface (whose seeds span the whole
+ * line at once), the number of solve passes, each followed by a fixed-point check
  * of every node (1..64, default 6), and the most steps one field's solve may
  * take (0: the default, 4,000,000).  A forward whose last check still finds
  * nodes that move, or in which a field reached the step cap, returns

@@ -38,7 +38,9 @@ def _compare(o, g, slot, src, tf):
 @pytest.mark.parametrize("phases", [(1,), (3,), (1, 2, 3, 4, 5)])
 def test_small_model_all_fields(oracle_lib, phases, window):
     """Every stage field of the five phases on the small model, with the
-    default schedule (no window) and with a half-cell time window."""
+    default schedule (no window for stages from the point source, 32 cells
+    for stages seeded along an interface) and with a half-cell time window
+    for every stage."""
     from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
     m = synth.small_model()
     o = oracle_lib.Oracle(m)
