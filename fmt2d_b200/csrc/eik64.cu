@@ -39,7 +39,7 @@ namespace {
 using namespace ev;
 
 // ---------------------------------------------------------------- field solve
-constexpr int kSolveThreads = 256;
+constexpr int kSolveThreads = 512;
 constexpr int kSolveWarps = kSolveThreads / 32;
 constexpr int kHalfWarps = kSolveThreads / 16;
 constexpr unsigned kLCap = 4096;          // entries of each list held in shared memory
