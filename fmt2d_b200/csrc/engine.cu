@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
+#include <thread>
 
 namespace fmt2d {
 
@@ -85,6 +86,11 @@ double seafloor_at(const Model& m, double px) {
 Engine::Engine(int device) : device_(device) {
   cudaSetDevice(device_);
   cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&ev_start_, cudaEventDisableTiming);
+  for (SolveLane& L : lanes_) {
+    cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+  }
   cudaMallocHost(&h_count_, 4 * sizeof(unsigned));
 }
 
@@ -92,6 +98,12 @@ Engine::~Engine() {
   cudaSetDevice(device_);
   fields_.clear();
   if (h_count_) cudaFreeHost(h_count_);
+  for (SolveLane& L : lanes_) {
+    L.free_all();
+    if (L.done) cudaEventDestroy(L.done);
+    if (L.st) cudaStreamDestroy(L.st);
+  }
+  if (ev_start_) cudaEventDestroy(ev_start_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -218,47 +230,70 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
   }
   stats_ = SolveStats();
   not_converged_ = false;
-  for (int level = 0; level <= 3; ++level) {
-    std::vector<std::pair<int, int>> items;
-    for (int tf = 1; tf <= 12; ++tf)
-      if ((need & (1u << tf)) && kTf[tf].level == level)
-        for (int s = 0; s < nsrc; ++s) items.emplace_back(s, tf);
-    if (items.empty()) continue;
-    std::string e = solve_level(items);
-    if (!e.empty()) return e;
+  // the stage chains (Pg -> Pg_ss, PsedP, PmP, Pg_ss2) are independent: each
+  // runs on its own stream, driven by its own host thread, after the work
+  // already queued on the context's stream and before anything queued on it
+  // later
+  bool active[kChains] = {};
+  for (int tf = 1; tf <= 12; ++tf)
+    if (need & (1u << tf)) active[chain_of(tf)] = true;
+  CK(cudaEventRecord(ev_start_, stream_));
+  std::string errs[kChains];
+  auto run_chain = [&](int c) {
+    cudaSetDevice(device_);
+    SolveLane& L = lanes_[c];
+    L.stats = SolveStats();
+    L.not_converged = false;
+    cudaStreamWaitEvent(L.st, ev_start_, 0);
+    for (int level = 0; level <= 3 && errs[c].empty(); ++level) {
+      std::vector<std::pair<int, int>> items;
+      for (int tf = 1; tf <= 12; ++tf)
+        if ((need & (1u << tf)) && kTf[tf].level == level && chain_of(tf) == c)
+          for (int s = 0; s < nsrc; ++s) items.emplace_back(s, tf);
+      if (!items.empty()) errs[c] = solve_level(L, items);
+    }
+    cudaEventRecord(L.done, L.st);
+  };
+  std::vector<std::thread> threads;
+  int nact = 0, last = -1;
+  for (int c = 0; c < kChains; ++c)
+    if (active[c]) {
+      ++nact;
+      last = c;
+    }
+  for (int c = 0; c < kChains; ++c)
+    if (active[c] && c != last) threads.emplace_back(run_chain, c);
+  if (last >= 0) run_chain(last);
+  for (std::thread& t : threads) t.join();
+  std::string err;
+  for (int c = 0; c < kChains; ++c) {
+    if (!active[c]) continue;
+    const SolveStats& q = lanes_[c].stats;
+    stats_.rounds = std::max(stats_.rounds, q.rounds);
+    stats_.round_ms = std::max(stats_.round_ms, q.round_ms);
+    stats_.steps_sum += q.steps_sum;
+    stats_.batches += q.batches;
+    stats_.final_passes += q.final_passes;
+    stats_.evals += q.evals;
+    stats_.writes += q.writes;
+    stats_.passed += q.passed;
+    stats_.unsettled += q.unsettled;
+    stats_.capped += q.capped;
+    stats_.launches += q.launches;
+    stats_.nodes += q.nodes;
+    for (int k = 0; k < 5; ++k) stats_.cycles[k] += q.cycles[k];
+    stats_.cut_evals += q.cut_evals;
+    stats_.cut_steps += q.cut_steps;
+    not_converged_ = not_converged_ || lanes_[c].not_converged;
+    cudaStreamWaitEvent(stream_, lanes_[c].done, 0);
+    if (err.empty() && !errs[c].empty()) err = errs[c];
   }
+  if (!err.empty()) return err;
   CK(cudaStreamSynchronize(stream_));
   return std::string();
 }
 
-Fld64 Engine::field_view(int src, int tf) const {
-  const Region& G = m_.reg[kTf[tf].reg];
-  const DevRegionStore& D = reg_[kTf[tf].reg];
-  const FieldStore& S = fields_[src][tf];
-  Fld64 f;
-  f.code = D.code.as<uint32_t>();
-  f.vel = D.vel64.as<double>();
-  f.izc = D.izc.as<int>();
-  f.ifx = D.iface_x.as<double>();
-  f.ifz = D.iface_z.as<double>();
-  f.H = G.H;
-  f.pitch = G.pitch;
-  f.z_lo = G.z_lo;
-  f.nx = m_.nx;
-  f.nz = m_.nz;
-  f.x0 = m_.x0;
-  f.dx = m_.dx;
-  f.tol = m_.tolerance;
-  f.T = S.T.as<double>();
-  f.G = S.G.as<double2>();
-  f.Gout = S.Gout.as<double2>();
-  f.fl = S.fl.as<uint8_t>();
-  f.seed = S.seed.as<double4>();
-  f.clock = S.clock.as<double>();
-  return f;
-}
-
-std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
+std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, int>>& items) {
   const int nf = (int)items.size();
   std::vector<Fld64> hf(nf);
   std::vector<int> up(nf, -1), hw;
@@ -274,18 +309,18 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   // solver scratch of the batch, per slot: staged time, gradient and flags,
   // pending time, start list, list and commit overflow, listed bitset
   const size_t words = (total + 31 * (size_t)nf + 31) / 32 + (size_t)nf;
-  d_sTn_.alloc(total * sizeof(double));
-  d_sGn_.alloc(total * sizeof(double2));
-  d_sfln_.alloc(total);
-  d_spend_.alloc(total * sizeof(double));
-  d_sclaim_.alloc(total * sizeof(unsigned long long));
-  d_slist_.alloc(total * sizeof(unsigned));
-  d_sover_.alloc(3 * total * sizeof(unsigned));
-  d_sinq_.alloc(3 * words * sizeof(unsigned));
-  d_scnt_.alloc((size_t)nf * 4 * sizeof(unsigned));
-  d_ctr_.alloc(kCtrN * sizeof(unsigned long long));
-  if (!d_sTn_.p || !d_sGn_.p || !d_sfln_.p || !d_spend_.p || !d_sclaim_.p || !d_slist_.p || !d_sover_.p ||
-      !d_sinq_.p || !d_scnt_.p || !d_ctr_.p)
+  L.sTn.alloc(total * sizeof(double));
+  L.sGn.alloc(total * sizeof(double2));
+  L.sfln.alloc(total);
+  L.spend.alloc(total * sizeof(double));
+  L.sclaim.alloc(total * sizeof(unsigned long long));
+  L.slist.alloc(total * sizeof(unsigned));
+  L.sover.alloc(3 * total * sizeof(unsigned));
+  L.sinq.alloc(3 * words * sizeof(unsigned));
+  L.scnt.alloc((size_t)nf * 4 * sizeof(unsigned));
+  L.ctr.alloc(kCtrN * sizeof(unsigned long long));
+  if (!L.sTn.p || !L.sGn.p || !L.sfln.p || !L.spend.p || !L.sclaim.p || !L.slist.p || !L.sover.p ||
+      !L.sinq.p || !L.scnt.p || !L.ctr.p)
     return "device allocation failed for the solver scratch";
   size_t base = 0, wbase = 0;
   int max_tiles = 0;
@@ -293,19 +328,19 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     const int s = items[i].first, tf = items[i].second;
     const DevRegionStore& D = reg_[kTf[tf].reg];
     hf[i] = field_view(s, tf);
-    hf[i].Tn = d_sTn_.as<double>() + base;
-    hf[i].Gn = d_sGn_.as<double2>() + base;
-    hf[i].fln = d_sfln_.as<uint8_t>() + base;
-    hf[i].pend = d_spend_.as<double>() + base;
-    hf[i].claim = d_sclaim_.as<unsigned long long>() + base;
-    hf[i].list_in = d_slist_.as<unsigned>() + base;
-    hf[i].over = d_sover_.as<unsigned>() + 3 * base;
-    hf[i].inq = d_sinq_.as<unsigned>() + wbase;
-    hf[i].wait = d_sinq_.as<unsigned>() + words + wbase;
-    hf[i].moving = d_sinq_.as<unsigned>() + 2 * words + wbase;
+    hf[i].Tn = L.sTn.as<double>() + base;
+    hf[i].Gn = L.sGn.as<double2>() + base;
+    hf[i].fln = L.sfln.as<uint8_t>() + base;
+    hf[i].pend = L.spend.as<double>() + base;
+    hf[i].claim = L.sclaim.as<unsigned long long>() + base;
+    hf[i].list_in = L.slist.as<unsigned>() + base;
+    hf[i].over = L.sover.as<unsigned>() + 3 * base;
+    hf[i].inq = L.sinq.as<unsigned>() + wbase;
+    hf[i].wait = L.sinq.as<unsigned>() + words + wbase;
+    hf[i].moving = L.sinq.as<unsigned>() + 2 * words + wbase;
     if (e64_tiles(hf[i]) > e64_tiles_max()) return "region too large for the eikonal solver";
     max_tiles = std::max(max_tiles, e64_tiles(hf[i]));
-    hf[i].cnt = d_scnt_.as<unsigned>() + 4 * (size_t)i;
+    hf[i].cnt = L.scnt.as<unsigned>() + 4 * (size_t)i;
     base += D.nslots;
     wbase += (D.nslots + 31) / 32;
     up[i] = kTf[tf].water_up;
@@ -319,25 +354,25 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
     if (tf == 5) hw.push_back(i);
   }
   std::string e;
-  if (!(e = put(d_fields_, hf, stream_)).empty()) return e;
-  if (!(e = put(d_up_, up, stream_)).empty()) return e;
-  if (!(e = put(d_step_, wstep, stream_)).empty()) return e;
-  unsigned long long* dctr = d_ctr_.as<unsigned long long>();
-  CK(cudaMemsetAsync(d_sinq_.p, 0, words * sizeof(unsigned), stream_));
-  CK(cudaMemsetAsync(d_scnt_.p, 0, (size_t)nf * 4 * sizeof(unsigned), stream_));
-  CK(cudaMemsetAsync(dctr, 0, kCtrN * sizeof(unsigned long long), stream_));
-  Fld64* dF = d_fields_.as<Fld64>();
-  e64_fill(dF, nf, max_slots, stream_);
-  ++stats_.launches;
+  if (!(e = put(L.fields, hf, L.st)).empty()) return e;
+  if (!(e = put(L.up, up, L.st)).empty()) return e;
+  if (!(e = put(L.step, wstep, L.st)).empty()) return e;
+  unsigned long long* dctr = L.ctr.as<unsigned long long>();
+  CK(cudaMemsetAsync(L.sinq.p, 0, words * sizeof(unsigned), L.st));
+  CK(cudaMemsetAsync(L.scnt.p, 0, (size_t)nf * 4 * sizeof(unsigned), L.st));
+  CK(cudaMemsetAsync(dctr, 0, kCtrN * sizeof(unsigned long long), L.st));
+  Fld64* dF = L.fields.as<Fld64>();
+  e64_fill(dF, nf, max_slots, L.st);
+  ++L.stats.launches;
   CK(cudaGetLastError());
   const int level = kTf[items[0].second].level;
   if (level == 0) {
     std::vector<double> sx(nf), sz(nf);
     for (int i = 0; i < nf; ++i) { sx[i] = src_x_[items[i].first]; sz[i] = src_z_[items[i].first]; }
-    if (!(e = put(d_sx_, sx, stream_)).empty()) return e;
-    if (!(e = put(d_sz_, sz, stream_)).empty()) return e;
-    e64_init_source(dF, d_sx_.as<double>(), d_sz_.as<double>(), nf, stream_);
-    ++stats_.launches;
+    if (!(e = put(L.sx, sx, L.st)).empty()) return e;
+    if (!(e = put(L.sz, sz, L.st)).empty()) return e;
+    e64_init_source(dF, L.sx.as<double>(), L.sz.as<double>(), nf, L.st);
+    ++L.stats.launches;
   } else {
     std::vector<Seed64> sd(nf);
     for (int i = 0; i < nf; ++i) {
@@ -360,12 +395,12 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
       d.reflect = I.reflect;
       d.target_side = I.target_side;
     }
-    if (!(e = put(d_seeds_, sd, stream_)).empty()) return e;
-    e64_seed_iface(dF, d_seeds_.as<Seed64>(), nf, m_.nx, stream_);
-    ++stats_.launches;
+    if (!(e = put(L.seeds, sd, L.st)).empty()) return e;
+    e64_seed_iface(dF, L.seeds.as<Seed64>(), nf, m_.nx, L.st);
+    ++L.stats.launches;
   }
-  e64_start(dF, nf, max_slots, d_step_.as<double>(), stream_);
-  stats_.launches += 2;
+  e64_start(dF, nf, max_slots, L.step.as<double>(), L.st);
+  L.stats.launches += 2;
   CK(cudaGetLastError());
   // solve, then check every node; nodes the check re-lists are solved again
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -376,18 +411,18 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
   }
   std::string err;
   std::vector<unsigned> hc((size_t)nf * 4);
-  cudaEventRecord(e0, stream_);
+  cudaEventRecord(e0, L.st);
   unsigned long long bad = 0;
   for (int pass = 0;; ++pass) {
-    e64_solve(dF, nf, max_slots, max_tiles, max_steps, dctr, stream_);
-    ++stats_.launches;
-    ++stats_.final_passes;
-    cudaMemsetAsync(d_sinq_.p, 0, words * sizeof(unsigned), stream_);
-    e64_verify(dF, nf, max_slots, stream_);
-    ++stats_.launches;
-    cudaError_t ce = cudaMemcpyAsync(hc.data(), d_scnt_.p, hc.size() * sizeof(unsigned),
-                                     cudaMemcpyDeviceToHost, stream_);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream_);
+    e64_solve(dF, nf, max_slots, max_tiles, max_steps, dctr, L.st);
+    ++L.stats.launches;
+    ++L.stats.final_passes;
+    cudaMemsetAsync(L.sinq.p, 0, words * sizeof(unsigned), L.st);
+    e64_verify(dF, nf, max_slots, L.st);
+    ++L.stats.launches;
+    cudaError_t ce = cudaMemcpyAsync(hc.data(), L.scnt.p, hc.size() * sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost, L.st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(L.st);
     if (ce != cudaSuccess) { err = std::string("eikonal solve: ") + cudaGetErrorString(ce); break; }
     bad = 0;
     unsigned capped = 0;
@@ -396,57 +431,57 @@ std::string Engine::solve_level(const std::vector<std::pair<int, int>>& items) {
       capped += hc[4 * (size_t)i + 2];
     }
     if (capped) {
-      stats_.capped += capped;
-      not_converged_ = true;
+      L.stats.capped += capped;
+      L.not_converged = true;
       err = "eikonal solve reached its step cap in " + std::to_string(capped) + " fields";
       break;
     }
     if (bad == 0 || pass + 1 >= max_passes) break;
   }
-  cudaEventRecord(e1, stream_);
+  cudaEventRecord(e1, L.st);
   cudaEventSynchronize(e1);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (!err.empty()) return err;
-  stats_.round_ms += ms;
+  L.stats.round_ms += ms;
   {
     unsigned long long c[kCtrN];
     CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
-    stats_.evals += c[kCtrEval];
-    stats_.writes += c[kCtrWrite];
-    stats_.passed += c[kCtrPass];
-    stats_.rounds += (long long)c[kCtrMaxSteps];
-    stats_.steps_sum += c[kCtrSteps];
-    for (int k = 0; k < 5; ++k) stats_.cycles[k] += (double)c[kCtrCycEval + k];
-    stats_.cut_evals += c[kCtrCut];
-    stats_.cut_steps += c[kCtrStepsCut];
+    L.stats.evals += c[kCtrEval];
+    L.stats.writes += c[kCtrWrite];
+    L.stats.passed += c[kCtrPass];
+    L.stats.rounds += (long long)c[kCtrMaxSteps];
+    L.stats.steps_sum += c[kCtrSteps];
+    for (int k = 0; k < 5; ++k) L.stats.cycles[k] += (double)c[kCtrCycEval + k];
+    L.stats.cut_evals += c[kCtrCut];
+    L.stats.cut_steps += c[kCtrStepsCut];
   }
   if (bad) {
-    stats_.unsettled += bad;
-    not_converged_ = true;
+    L.stats.unsettled += bad;
+    L.not_converged = true;
     return "eikonal solve did not reach its fixed point (" + std::to_string(bad) +
            " nodes still move after " + std::to_string(max_passes) + " passes)";
   }
-  e64_finish(dF, nf, max_slots, d_up_.as<int>(), stream_);
-  stats_.launches += 2;
+  e64_finish(dF, nf, max_slots, L.up.as<int>(), L.st);
+  L.stats.launches += 2;
   CK(cudaGetLastError());
   if (!hw.empty()) {
-    if (!(e = put(d_which_, hw, stream_)).empty()) return e;
-    d_scratch_.alloc(hw.size() * (size_t)m_.nx * sizeof(double));
+    if (!(e = put(L.which, hw, L.st)).empty()) return e;
+    L.hw.alloc(hw.size() * (size_t)m_.nx * sizeof(double));
     const double dx_if = m_.xpos[1] - m_.xpos[0];
     e64_headwave(dF, hw_slot_.as<int>(), hw_v_.as<double>(), dx_if, m_.nx,
-                 d_scratch_.as<double>(), d_which_.as<int>(), (int)hw.size(), stream_);
-    ++stats_.launches;
+                 L.hw.as<double>(), L.which.as<int>(), (int)hw.size(), L.st);
+    ++L.stats.launches;
     CK(cudaGetLastError());
   }
-  CK(cudaStreamSynchronize(stream_));
+  CK(cudaStreamSynchronize(L.st));
   for (int i = 0; i < nf; ++i) {
     fields_[items[i].first][items[i].second].solved = true;
-    stats_.nodes += m_.reg[kTf[items[i].second].reg].nnode;
+    L.stats.nodes += m_.reg[kTf[items[i].second].reg].nnode;
   }
-  ++stats_.batches;
+  ++L.stats.batches;
   return std::string();
 }
 

@@ -76,6 +76,29 @@ struct SolveStats {
   unsigned long long cut_steps = 0;     // steps that evaluated such a node
 };
 
+// Stage chains solved concurrently: a stage's chain is that of its level-0
+// ancestor (Pg with Pg_ss, PsedP, PmP, Pg_ss2).
+constexpr int kChains = 4;
+inline int chain_of(int tf) {
+  static const int c[13] = {0, 0, 1, 1, 2, 2, 0, 0, 0, 3, 3, 3, 3};
+  return c[tf];
+}
+
+// A stream and the solver scratch of one stage chain.
+struct SolveLane {
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf fields, up, step, sx, sz, seeds, which, hw, ctr;
+  DevBuf sTn, sGn, sfln, spend, sclaim, slist, sover, sinq, scnt;
+  SolveStats stats;
+  bool not_converged = false;
+  void free_all() {
+    for (DevBuf* b : {&fields, &up, &step, &sx, &sz, &seeds, &which, &hw, &ctr, &sTn, &sGn, &sfln,
+                      &spend, &sclaim, &slist, &sover, &sinq, &scnt})
+      b->free_();
+  }
+};
+
 class Engine {
  public:
   explicit Engine(int device);
@@ -115,7 +138,7 @@ class Engine {
   int nsrc() const { return (int)fields_.size(); }
 
  private:
-  std::string solve_level(const std::vector<std::pair<int, int>>& items);
+  std::string solve_level(SolveLane& L, const std::vector<std::pair<int, int>>& items);
   std::string upload_trace_tables();
   void ensure_sources(int nsrc);
   Fld64 field_view(int src, int tf) const;
@@ -128,9 +151,9 @@ class Engine {
   DevBuf hw_slot_, hw_v_;
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
-  DevBuf d_fields_, d_seeds_, d_sx_, d_sz_, d_scratch_, d_which_, d_up_, d_step_, d_ctr_;
   DevBuf export_;             // region-order copy of a field being read back
-  DevBuf d_sTn_, d_sGn_, d_sfln_, d_spend_, d_sclaim_, d_slist_, d_sover_, d_sinq_, d_scnt_;
+  SolveLane lanes_[kChains];
+  cudaEvent_t ev_start_ = nullptr;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
       d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
   int npick_ = -1, rows_ = 0;
