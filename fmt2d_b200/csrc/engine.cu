@@ -293,6 +293,33 @@ std::string Engine::forward(const double* sx, int nsrc, int phase_mask) {
   return std::string();
 }
 
+Fld64 Engine::field_view(int src, int tf) const {
+  const Region& G = m_.reg[kTf[tf].reg];
+  const DevRegionStore& D = reg_[kTf[tf].reg];
+  const FieldStore& S = fields_[src][tf];
+  Fld64 f;
+  f.code = D.code.as<uint32_t>();
+  f.vel = D.vel64.as<double>();
+  f.izc = D.izc.as<int>();
+  f.ifx = D.iface_x.as<double>();
+  f.ifz = D.iface_z.as<double>();
+  f.H = G.H;
+  f.pitch = G.pitch;
+  f.z_lo = G.z_lo;
+  f.nx = m_.nx;
+  f.nz = m_.nz;
+  f.x0 = m_.x0;
+  f.dx = m_.dx;
+  f.tol = m_.tolerance;
+  f.T = S.T.as<double>();
+  f.G = S.G.as<double2>();
+  f.Gout = S.Gout.as<double2>();
+  f.fl = S.fl.as<uint8_t>();
+  f.seed = S.seed.as<double4>();
+  f.clock = S.clock.as<double>();
+  return f;
+}
+
 std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, int>>& items) {
   const int nf = (int)items.size();
   std::vector<Fld64> hf(nf);
