@@ -12,18 +12,29 @@ eikonal time fields, solved through the library's public entry point.
 * e2e    : the same metric through the public API from host buffers: model
            upload (host arrays -> device), the forward solve, and the read-back
            of every terminal-stage traveltime field to host memory.
-* roofline: the step kernel (k_step) against the measured HBM bandwidth, with
-           the algorithmic traffic of one field: 36 B per region node (FP64
-           time and gradient written once, FP64 velocity and the 4-byte node
-           code read once), over the device time of the step loops.
+* roofline: the field solve (k_solve) against the measured HBM bandwidth,
+           with the algorithmic traffic of one field: 16 B per region node
+           (4 B slowness read, 4 B time and 8 B gradient written, the FP32
+           figure of the traveltime contract; the FP64 fields this build keeps
+           move 36 B per node, reported beside it), over the forward's device
+           time (the solves of independent stage chains overlap).
+* max_err_ms: the largest traveltime difference, over every reached node of
+           every field of one source, against the FP64 heap fast marching
+           restatement (oracle/, the checker); reached sets must agree.
+* rays, lsqr: ray backtrace + Frechet rows of every Pg and PmP pick of the
+           model (picks/s, device-timed), and the LSQR solve on those rows
+           (s per LSQR iteration).
 * cpu_baseline: the FP64 CPU restatement of the reference algorithm (oracle/)
-           on the host cores, over a bounded sample of the same workload.
+           on the host cores, over a bounded sample of the same workload
+           (pool warmed first, median of 3 timed repetitions).
 * --impl reference: the CPU restatement timed on all host cores (the reference
            Fortran cannot be built here: no Fortran compiler in the image).
 
-Multi-GPU: one process per GPU (torchrun); every rank solves its own copy of
-the workload (independent source sets), no collective on the data path
-(weak scaling); the step time is the max over ranks.
+Multi-GPU: one process per GPU (torchrun).  Sources are independent, so the
+ranks share out a larger source set: rank r solves the model's 30 OBS
+positions shifted by r/N of the OBS spacing (30 N distinct sources in all),
+with no collective on the data path (weak scaling); the step time is the max
+over ranks.
 """
 from __future__ import annotations
 
@@ -80,15 +91,33 @@ def _cpu_worker(args):
     return time.perf_counter() - t0
 
 
-def cpu_fields_per_s(nsrc: int, procs: int, reps: int = 1):
-    """Fields/s of the CPU restatement over `nsrc` sources on `procs` processes,
-    the processes' mean single-core rate and the wall times."""
+def _cpu_fields_of_source(args):
+    """The checker: the CPU restatement's traveltimes of every field of one
+    source (FP64 heap fast marching)."""
+    sx, phases = args
+    _cpu_init()
+    from fmt2d_b200.api import fields_of, phase_mask
+    o = _CPU_STATE["o"]
+    mask = phase_mask(phases)
+    o.forward(0, float(sx), mask)
+    return {tf: o.field(0, tf)[0] for tf in fields_of(mask)}
+
+
+def cpu_fields_per_s(nsrc: int, procs: int, reps: int = 3, check_x=None):
+    """Fields/s of the CPU restatement over `nsrc` sources on `procs` processes
+    (the pool is warmed by one untimed pass; median of `reps` timed passes),
+    the processes' mean single-core rate, the wall times and, for check_x,
+    the checker's fields of a source at that x."""
     from fmt2d_b200.api import fields_of, phase_mask
     nf_src = len(fields_of(phase_mask(PHASES)))
     ctx = mp.get_context("spawn")
     chunks = [list(range(i, nsrc, procs)) for i in range(procs)]
     chunks = [c for c in chunks if c]
+    checked = None
     with ctx.Pool(len(chunks), initializer=_cpu_init) as pool:
+        pool.map(_cpu_worker, [(c[:1], PHASES) for c in chunks])
+        if check_x is not None:
+            checked = pool.map(_cpu_fields_of_source, [(check_x, PHASES)])[0]
         walls, rates = [], []
         for _ in range(reps):
             t0 = time.perf_counter()
@@ -96,7 +125,7 @@ def cpu_fields_per_s(nsrc: int, procs: int, reps: int = 1):
             walls.append(time.perf_counter() - t0)
             rates += [len(c) * nf_src / t for c, t in zip(chunks, secs) if t > 0]
     one = float(np.mean(rates)) if rates else 0.0
-    return nsrc * nf_src / float(np.median(walls)), len(chunks), walls, one
+    return nsrc * nf_src / float(np.median(walls)), len(chunks), walls, one, checked
 
 
 # ---------------------------------------------------------------- clocks
@@ -162,6 +191,19 @@ def measured_peak_hbm():
     except (OSError, ValueError):
         pass
     return 6650.0, "fallback"
+
+
+# DRAM bytes (read + write) per region node of the field solve (k_solve), from
+# an ncu capture of one launch (None until one is summarised under profiles/)
+K_SOLVE_DRAM_BYTES_PER_NODE = None
+
+
+def traffic_per_step(nodes_step: float):
+    """DRAM traffic of the step's field solves, scaled from the captured
+    launch by region nodes (the solve's traffic grows with the nodes)."""
+    if K_SOLVE_DRAM_BYTES_PER_NODE is None:
+        return None
+    return round(K_SOLVE_DRAM_BYTES_PER_NODE * nodes_step)
 
 
 def dist_setup(n_gpus):
@@ -241,29 +283,110 @@ def run_reference(args, world, rank):
     print(json.dumps(out), flush=True)
 
 
+def source_set(m, rank: int, world: int) -> np.ndarray:
+    """Sources of one rank: the model's OBS positions shifted by rank/world of
+    the OBS spacing (on grid nodes), so the ranks solve distinct sources."""
+    x = np.asarray(m.obs_x, dtype=np.float64)
+    if world > 1 and x.size > 1:
+        x = x + rank * (x[1] - x[0]) / world
+        x = np.round(x / m.dx) * m.dx
+        x = np.clip(x, m.xpos[1], m.xpos[-2])
+    return x
+
+
+def max_error_ms(g, checked, mask):
+    """Largest |T_device - T_checker| (ms) over the nodes both reach, and the
+    number of nodes reached by one side only, over every field of source 0."""
+    from fmt2d_b200.api import fields_of
+    worst, reach_diff = 0.0, 0
+    for tf in fields_of(mask):
+        To = checked[tf]
+        Tg = g.field(0, tf)[0]
+        ro, rg = To < 1e19, Tg < 1e19
+        reach_diff += int((ro != rg).sum())
+        both = ro & rg
+        if both.any():
+            worst = max(worst, float(np.abs(To[both] - Tg[both]).max()))
+    return worst * 1e3, reach_diff
+
+
+def timed_on(stream, fn):
+    """Run fn and return (its result, device ms between events on stream)."""
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    out = fn()
+    b.record(stream)
+    b.synchronize()
+    return out, a.elapsed_time(b)
+
+
+def rays_and_lsqr(g, m, stream):
+    """Ray backtrace + Frechet rows of every pick of the model on the fields
+    of the last forward (picks/s), then the damped, smoothed LSQR solve on the
+    selected rows (s per LSQR iteration).  Observed times are the computed
+    ones plus seeded 40 ms Gaussian noise (config-1 pick noise)."""
+    from fmt2d_b200.api import select_data
+    P = m.picks
+    src = P[:, 0].astype(np.int32)
+    ph = P[:, 1].astype(np.int32)
+    rx, rz = P[:, 2].copy(), P[:, 3].copy()
+    g.trace(src, ph, rx, rz)                       # warm (tables, buffers)
+    (t, valid, nnz), tr_ms = timed_on(stream, lambda: g.trace(src, ph, rx, rz))
+    rp, gi, gv = g.frechet_rows()
+    rng = np.random.default_rng(1)
+    obs = np.where(valid, t + rng.normal(0.0, 0.040, t.size), -1.0)
+    _, nvp, npar = g.inv_index()
+    mv = np.ones(npar)
+    srp, sgi, sgv, res, wt, _ = select_data(ph, obs, t, valid, rp, gi, gv, mv, crit_chi=1.0)
+    nd = srp.size - 1
+    g.set_frechet(nd, npar, srp, sgi, sgv)
+    gtg = g.gtg_diag()
+    eps_min = max(1e-6, 1e-4 * float(gtg.max()))
+    iters = 100
+    g.lsqr(res, np.zeros(npar), gtg, wdv=1.0, wdv_iface=1.0, w_smooth=10.0,
+           w_smooth_iface=10.0, eps_min=0.0, max_iter=8)  # warm (graph, buffers)
+    _, it, _, _, _ = g.lsqr(res, np.zeros(npar), gtg, wdv=1.0, wdv_iface=1.0, w_smooth=10.0,
+                            w_smooth_iface=10.0, eps_min=eps_min, max_iter=iters)
+    ls = g.lsqr_stats()
+    rays = {"value": round(P.shape[0] / (tr_ms / 1e3), 1), "unit": "picks/s",
+            "picks": int(P.shape[0]), "valid": int(valid.sum()), "frechet_nnz": int(nnz),
+            "ms": round(tr_ms, 3), "note": "fmt2d_trace, device-timed, fields resident"}
+    lsqr = {"value": round(ls["ms"] / 1e3 / max(it, 1), 6), "unit": "s per LSQR iteration",
+            "iterations": int(it), "ndata": int(nd), "nparm": int(npar), "nnz": int(sgi.size),
+            "ms": round(ls["ms"], 3), "smooth_type": 1,
+            "note": "fmt2d_lsqr, damping 1, Laplacian 10, device-timed"}
+    return rays, lsqr
+
+
 def run_ours(args, world, rank, local):
-    cpu = None
+    from fmt2d_b200 import synth
+    from fmt2d_b200.api import fields_of, phase_mask
+    m = synth.config(1)
+    src = source_set(m, rank, world)
+    mask = phase_mask(PHASES)
+    cpu, checked = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        # before the first CUDA call: the CPU restatement on the host cores
+        # before the first CUDA call: the CPU restatement on the host cores,
+        # and the checker's fields of source 0
         cores = os.cpu_count() or 1
         nsrc = min(30, max(4, cores))
         procs = min(cores, nsrc)
-        v, used, walls, one = cpu_fields_per_s(nsrc, procs)
+        v, used, walls, one, checked = cpu_fields_per_s(nsrc, procs, reps=3,
+                                                        check_x=float(src[0]))
         cpu = {"value": round(v, 3), "unit": "fields/s", "cores": used, "kind": "port",
                "sample": f"{nsrc} sources x Pg+PmP stages of the same model, FP64 heap fast "
-                         f"marching, {used} processes, {walls[0]:.1f} s wall",
+                         f"marching, {used} processes, pool warmed, median of "
+                         f"{len(walls)} passes ({', '.join(f'{w:.1f}' for w in walls)} s wall)",
                "single_core": {"value": round(one, 3), "unit": "fields/s",
                                "sample": "mean rate of one process (one core) in that run"}}
     import torch
-    from fmt2d_b200 import synth
-    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask, TF_REGION
+    from fmt2d_b200.api import Fmt2d, TF_REGION
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    m = synth.config(1)
     g = Fmt2d(local).upload(m)
     stream = torch.cuda.ExternalStream(g.stream(), device=dev)
-    src = np.asarray(m.obs_x, dtype=np.float64)
-    mask = phase_mask(PHASES)
     nf = len(fields_of(mask)) * src.size
     terminal = [1, 5]          # last stage of Pg and of PmP (ray tracing starts there)
 
@@ -271,8 +394,9 @@ def run_ours(args, world, rank, local):
         g.forward(src, PHASES)
     torch.cuda.synchronize()
 
-    # ---- device-resident timing
-    solve_ms, launches, nodes = 0.0, 0, 0
+    # ---- device-resident timing (fmt2d_forward raises Fmt2dNotConverged if a
+    # field does not reach its fixed point; the counters are checked too)
+    launches, nodes, capped, unsettled = 0, 0, 0, 0
     with ClockSampler(local) as clk:
         barrier(world)
         torch.cuda.synchronize()
@@ -282,17 +406,28 @@ def run_ours(args, world, rank, local):
         for _ in range(args.steps):
             g.forward(src, PHASES)
             st = g.stats()
-            solve_ms += st["solve_ms"]
             launches += st["launches"]
             nodes += st["nodes"]
+            capped += st["capped"]
+            unsettled += st["unsettled"]
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
         barrier(world)
         ms = e0.elapsed_time(e1)
+    if capped or unsettled:
+        raise RuntimeError(f"forward not converged: capped={capped} unsettled={unsettled}")
     ms = max_over_ranks(ms, world, dev)
     step_ms = ms / args.steps
     value = world * nf / (step_ms / 1e3)
+    solver = {k: st[k] for k in ("steps", "steps_all", "evals", "writes", "passes")}
+
+    err_ms, reach_diff = (None, None)
+    if checked is not None:
+        err_ms, reach_diff = max_error_ms(g, checked, mask)
+        if err_ms > 0.5 or reach_diff > 2 * len(checked):
+            raise RuntimeError(f"traveltime error {err_ms:.4f} ms, reach differs at "
+                               f"{reach_diff} nodes")
 
     # ---- end to end through the public API from host buffers
     bufs = {}
@@ -300,6 +435,7 @@ def run_ours(args, world, rank, local):
         n = g.region_nnode(TF_REGION[tf])
         bufs[tf] = np.zeros(n)
     h2d = sum(np.asarray(a).nbytes for a in (m.xpos, m.topo, m.zrel, m.vel, m.sed_z, m.moho_z))
+    h2d += src.nbytes
     d2h = sum(src.size * bufs[tf].nbytes for tf in terminal)
 
     def e2e_step():
@@ -321,31 +457,34 @@ def run_ours(args, world, rank, local):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world, dev)
     e2e_value = world * nf / e2e_s
 
+    # ---- rays + Frechet rows and LSQR on the same fields (every rank, the
+    # same steps, outside the timed region)
+    try:
+        g.forward(src, PHASES)
+        rays, lsqr = rays_and_lsqr(g, m, stream)
+    except Exception as ex:  # the eikonal line is the result; report why these are absent
+        rays = lsqr = {"unavailable": str(ex)[:200]}
+
     # ---- the plain form, one source (its stage solves) per fmt2d_forward call,
-    # on a few sources: the denominator of "batched vs plain"; outside the
-    # timed region and never allowed to cost the main line
+    # on a few sources: the denominator of "batched vs plain"
     try:
         k = int(min(3, src.size))
         torch.cuda.synchronize()
-        p0 = torch.cuda.Event(enable_timing=True)
-        p1 = torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        for i in range(k):
-            g.forward(src[i:i + 1], PHASES)
-        p1.record(stream)
-        p1.synchronize()
-        plain_ms = p0.elapsed_time(p1)
+        _, plain_ms = timed_on(stream, lambda: [g.forward(src[i:i + 1], PHASES)
+                                                for i in range(k)])
         plain = {"value": round(k * len(fields_of(mask)) / (plain_ms / 1e3), 3),
                  "unit": "fields/s", "sources_timed": k,
                  "note": "one source per fmt2d_forward call, device-timed"}
-    except Exception as ex:  # the batched line is the result; report why this is absent
+    except Exception as ex:
         plain = {"unavailable": str(ex)[:200]}
 
     if rank != 0:
+        g.close()
         return
     peak, peak_kind = measured_peak_hbm()
-    alg_bytes = 36.0 * nodes / args.steps          # per step, all fields
-    achieved = alg_bytes / (solve_ms / args.steps / 1e3) / 1e9 if solve_ms > 0 else None
+    nodes_step = nodes / args.steps
+    alg_bytes = 16.0 * nodes_step                  # per step, all fields
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
     out = {"metric": METRIC, "value": round(value, 3), "unit": "fields/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -353,15 +492,21 @@ def run_ours(args, world, rank, local):
            "config": {"workload": WORKLOAD, "grid": "2001x401", "sources_per_gpu": int(src.size),
                       "fields_per_gpu": nf, "l2": "field data per step (> 1 GB) exceeds L2",
                       "parallelism": f"sources x {world} gpus, independent"},
+           "max_err_ms": round(err_ms, 5) if err_ms is not None else None,
+           "reach_diff_nodes": reach_diff,
+           "converged": {"capped": int(capped), "unsettled": int(unsettled)},
            "e2e": {"value": round(e2e_value, 3), "unit": "fields/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(d2h), "includes": "model upload, forward, "
                    "terminal-stage traveltime read-back"},
-           "roofline": {"bound": "hbm", "kernel": "k_step",
-                        "achieved": round(achieved, 3) if achieved else None,
-                        "peak": peak, "unit": "GB/s",
-                        "frac": round(achieved / peak, 6) if achieved else None,
-                        "peak_kind": peak_kind, "traffic": None,
-                        "algorithmic_bytes_per_step": alg_bytes},
+           "roofline": {"bound": "hbm", "kernel": "k_solve",
+                        "achieved": round(achieved, 4), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 7), "peak_kind": peak_kind,
+                        "traffic": traffic_per_step(nodes_step),
+                        "algorithmic_bytes_per_step": alg_bytes,
+                        "bytes_per_node": 16, "fp64_bytes_per_node": 36,
+                        "fp64_frac": round(36.0 * nodes_step / (step_ms / 1e3) / 1e9 / peak, 7)},
+           "solver": solver,
+           "rays": rays, "lsqr": lsqr,
            "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "cpu_baseline": cpu}

@@ -28,3 +28,26 @@ def test_peak_lookup(tmp_path, monkeypatch):
     assert bench.measured_peak_hbm() == (6650.0, "fallback")
     (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6438.5}))
     assert bench.measured_peak_hbm() == (6438.5, "measured")
+
+
+def test_source_sets_and_error_check():
+    import numpy as np
+    from fmt2d_b200 import synth
+    m = synth.config(1)
+    one = bench.source_set(m, 0, 1)
+    assert np.array_equal(one, m.obs_x)
+    shards = [bench.source_set(m, r, 4) for r in range(4)]
+    allx = np.concatenate(shards)
+    assert allx.size == 120 and np.unique(np.round(allx, 6)).size == 120
+    assert all(s.min() >= m.xpos[1] and s.max() <= m.xpos[-2] for s in shards)
+
+    class FakeCtx:                      # device fields = checker + 0.2 ms, one node unreached
+        def field(self, s, tf):
+            T = checked[tf] + 2e-4
+            T[0] = 1e20
+            return T, None, None
+
+    checked = {1: np.linspace(0.0, 5.0, 50), 4: np.linspace(0.0, 7.0, 40),
+               5: np.linspace(1.0, 9.0, 40)}
+    err, diff = bench.max_error_ms(FakeCtx(), checked, 0b101)
+    assert abs(err - 0.2) < 1e-9 and diff == 3

@@ -1,7 +1,8 @@
 """The multi-process path of bench.py on the host: two ranks launched by
 torch.distributed.run (as for `bench.py --gpus 2`), the process group on
-gloo, the step time reduced as the max over ranks, and the reference arm
-printing its one JSON line from rank 0 only."""
+gloo, the step time reduced as the max over ranks, the sources shared out
+(each rank its own 30), and the reference arm printing its one JSON line
+from rank 0 only."""
 import json
 import os
 import socket
@@ -36,6 +37,9 @@ def test_max_over_ranks_gloo(tmp_path):
     assert [d["rank"] for d in rows] == [0, 1]
     assert all(d["world"] == 2 and d["backend"] == "gloo" for d in rows)
     assert all(d["max_ms"] == 15.0 for d in rows)
+    # each rank solves its own sources: 30 per rank, 60 distinct in all
+    a, b = (set(round(x, 6) for x in d["src"]) for d in rows)
+    assert len(a) == len(b) == 30 and not (a & b)
 
 
 def test_reference_arm_two_ranks():
