@@ -360,6 +360,43 @@ def rays_and_lsqr(g, m, stream):
     return rays, lsqr
 
 
+def inversion_iterations(local, n_iter: int = 2):
+    """Seconds per outer inversion iteration on the 2001x401 model (the
+    lsqr_inversion2d loop body, fmt2d_b200.inversion): observed times are the
+    checkerboard model's (device forward + rays, seeded 40 ms noise), the
+    inversion starts from the smooth model with a flat Moho; fixed damping 1,
+    Laplacian smoothing 10, alternating velocity / interface schedule.  Each
+    iteration: forward + rays + Frechet rows, selection, LSQR, line-search
+    forwards with model steps."""
+    from fmt2d_b200 import synth
+    from fmt2d_b200.api import Fmt2d
+    from fmt2d_b200.inversion import Inversion, InversionParams
+    true, start = synth.config(1), synth.start_model(1)
+    P = true.picks
+    g = Fmt2d(local).upload(true)
+    g.forward(true.obs_x, PHASES)
+    t, valid, _ = g.trace(P[:, 0].astype(np.int32), P[:, 1].astype(np.int32), P[:, 2], P[:, 3])
+    g.close()
+    rng = np.random.default_rng(1)
+    obs = np.where(valid, t + rng.normal(0.0, 0.040, t.size), -1.0)
+    g = Fmt2d(local).upload(start)
+    inv = Inversion(g, start.obs_x, P, obs,
+                    InversionParams(phases=PHASES, lam_damp=1.0, lam_smooth=10.0,
+                                    lam_smooth_iface=10.0, crit_chi=1.0, alt_inv_mode=-1))
+    rows = []
+    for _ in range(n_iter):
+        r = inv.iteration()
+        rows.append({"s": round(r.seconds, 3), "rms_orig_ms": round(1e3 * r.rms_orig, 3),
+                     "rms_new_ms": round(1e3 * r.rms_new, 3), "step": r.step, "ndata": r.ndata,
+                     "forwards": r.forwards, "lsqr_solves": r.lsqr_solves,
+                     "phases_s": {k: round(v, 3) for k, v in r.phases_s.items()}})
+    g.close()
+    return {"value": round(float(np.mean([x["s"] for x in rows])), 3),
+            "unit": "s per inversion iteration", "iterations": rows,
+            "workload": "2001x401, 30 OBS, Pg+PmP, 29344 picks, start: smooth model, flat Moho",
+            "note": "wall clock through the public API, 1 GPU"}
+
+
 def run_ours(args, world, rank, local):
     from fmt2d_b200 import synth
     from fmt2d_b200.api import fields_of, phase_mask
@@ -465,6 +502,15 @@ def run_ours(args, world, rank, local):
     except Exception as ex:  # the eikonal line is the result; report why these are absent
         rays = lsqr = {"unavailable": str(ex)[:200]}
 
+    # ---- s per inversion iteration (rank 0 of a 1-GPU run; outside the
+    # timed region)
+    inversion = None
+    if world == 1 and not args.no_inversion:
+        try:
+            inversion = inversion_iterations(local)
+        except Exception as ex:
+            inversion = {"unavailable": str(ex)[:200]}
+
     # ---- the plain form, one source (its stage solves) per fmt2d_forward call,
     # on a few sources: the denominator of "batched vs plain"
     try:
@@ -506,7 +552,7 @@ def run_ours(args, world, rank, local):
                         "bytes_per_node": 16, "fp64_bytes_per_node": 36,
                         "fp64_frac": round(36.0 * nodes_step / (step_ms / 1e3) / 1e9 / peak, 7)},
            "solver": solver,
-           "rays": rays, "lsqr": lsqr,
+           "rays": rays, "lsqr": lsqr, "inversion": inversion,
            "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "cpu_baseline": cpu}
@@ -521,6 +567,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-inversion", action="store_true",
+                    help="skip the s-per-inversion-iteration leg")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-core arm: rank 0 alone runs it, the other ranks exit without work

@@ -109,6 +109,10 @@ def lib():
                                      C.c_void_p, P(C.c_int), P(C.c_double), P(C.c_double),
                                      P(C.c_double)]
     L.fmt2d_lsqr_stats.argtypes = [V, P(C.c_double), P(C.c_int)]
+    L.fmt2d_set_smoothing.argtypes = [V, C.c_double, C.c_double, C.c_double, C.c_void_p]
+    L.fmt2d_model_velocity.argtypes = [V, C.c_void_p]
+    L.fmt2d_model_interface.argtypes = [V, C.c_int, C.c_void_p]
+    L.fmt2d_update_model.argtypes = [V, C.c_void_p, C.c_void_p]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int
     _lib = L

@@ -125,6 +125,32 @@ class Fmt2d:
                                             C.byref(x0)), "fmt2d_model_info")
         self.nx, self.nz, self.dx, self.x0 = nx.value, nz.value, dx.value, x0.value
         self.model = m
+        self.iface_inv = int(iface_inv)
+        return self
+
+    def velocity(self) -> np.ndarray:
+        """Propagation-grid velocity (nz, nx) of the current model."""
+        v = np.zeros(self.nx * self.nz)
+        self._check(self.L.fmt2d_model_velocity(self.h, N.ptr(v)), "fmt2d_model_velocity")
+        return v.reshape(self.nz, self.nx)
+
+    def interface(self, k: int) -> np.ndarray:
+        """Node depths of interface k (1..5)."""
+        z = np.zeros(self.nx)
+        self._check(self.L.fmt2d_model_interface(self.h, int(k), N.ptr(z)),
+                    "fmt2d_model_interface")
+        return z
+
+    def update_model(self, vel=None, iface_z=None):
+        """A model step (fmt2d_update_model): new propagation-grid velocity
+        (nz, nx) and / or new depths of the inverted interface."""
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).ravel()
+        z = None if iface_z is None else np.ascontiguousarray(iface_z, dtype=np.float64)
+        if v is not None and v.size != self.nx * self.nz:
+            raise ValueError("vel must have nz * nx entries")
+        if z is not None and z.size != self.nx:
+            raise ValueError("iface_z must have nx entries")
+        self._check(self.L.fmt2d_update_model(self.h, N.ptr(v), N.ptr(z)), "fmt2d_update_model")
         return self
 
     def region_nodes(self, r: int):
@@ -274,6 +300,19 @@ class Fmt2d:
         self._check(self.L.fmt2d_gtg_diag(self.h, N.ptr(out)), "fmt2d_gtg_diag")
         return out
 
+    def set_smoothing(self, mvscale, corr_x=0.0, corr_z=0.0, corr_x_iface=0.0):
+        """Gaussian smoothing operators of the smooth_type 2/3 LSQR layouts
+        (fmt2d_set_smoothing): R_h (corr_x > 0), R_v (corr_z > 0) and the
+        interface R_h (corr_x_iface > 0), mvscale folded in."""
+        mv = np.ascontiguousarray(mvscale, dtype=np.float64)
+        npar = self.inv_index()[2]
+        if mv.size != npar:
+            raise ValueError(f"mvscale has {mv.size} entries, the model has {npar} parameters")
+        self._check(self.L.fmt2d_set_smoothing(self.h, float(corr_x), float(corr_z),
+                                               float(corr_x_iface), N.ptr(mv)),
+                    "fmt2d_set_smoothing")
+        return self
+
     def lsqr(self, residual, dm_sum=None, gtg_diag=None, *, wdv=0.0, wdv_iface=0.0,
              w_smooth=0.0, w_smooth_iface=0.0, eps_min=0.0, max_iter=2000, smooth_type=1):
         """run_lsqr on the current G; returns (dm, iters, rnorm, bnorm, test2)."""
@@ -290,7 +329,8 @@ class Fmt2d:
 
     def lsqr_damped(self, residual, dm_sum=None, gtg_diag=None, mvscale=None, *,
                     lam_damp=0.0, lam_damp_iface=0.0, target_dv=0.0, target_dd=0.0,
-                    w_smooth=0.0, w_smooth_iface=0.0, eps_min=0.0, max_iter=2000):
+                    w_smooth=0.0, w_smooth_iface=0.0, eps_min=0.0, max_iter=2000,
+                    smooth_type=1):
         """lsqr_inversion2d's damping choice (src/inversion2d.f90:533-739):
         a fixed damping weight (lam_damp > 0) or tomo2d's auto damping towards
         the RMS velocity change target_dv and depth change target_dd, each
@@ -308,7 +348,7 @@ class Fmt2d:
         def solve(wdv, wdi):
             return self.lsqr(residual, dm_sum, gtg_diag, wdv=wdv, wdv_iface=wdi,
                              w_smooth=w_smooth, w_smooth_iface=w_smooth_iface,
-                             eps_min=eps_min, max_iter=max_iter)[0]
+                             eps_min=eps_min, max_iter=max_iter, smooth_type=smooth_type)[0]
 
         return damping_search(solve, dm_sum, gtg_diag, mvscale, eps_min, nvp,
                               lam_damp=lam_damp, lam_damp_iface=lam_damp_iface,

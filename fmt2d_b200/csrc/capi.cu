@@ -2,6 +2,7 @@
 #include "../../include/fmt2d_gpu.h"
 #include "engine.h"
 #include "lsqr.h"
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -89,6 +90,38 @@ int fmt2d_model_info(fmt2d_ctx* ctx, int* nx, int* nz, double* dx, double* x0) {
   if (nz) *nz = m.nz;
   if (dx) *dx = m.dx;
   if (x0) *x0 = m.x0;
+  return FMT2D_OK;
+}
+
+int fmt2d_model_velocity(fmt2d_ctx* ctx, double* vel) {
+  if (!ctx || !vel) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  std::copy(ctx->model.vel.begin(), ctx->model.vel.end(), vel);
+  return FMT2D_OK;
+}
+
+int fmt2d_model_interface(fmt2d_ctx* ctx, int k, double* z) {
+  if (!ctx || !z || k < 1 || k > 5) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  std::copy(ctx->model.ifc[k].z.begin(), ctx->model.ifc[k].z.end(), z);
+  return FMT2D_OK;
+}
+
+int fmt2d_update_model(fmt2d_ctx* ctx, const double* vel, const double* iface_z) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  fmt2d::Model next = ctx->model;
+  std::string e = fmt2d::update_model(next, vel, iface_z);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_MODEL, e);
+  ctx->has_model = false;
+  ctx->model = std::move(next);
+  if (ctx->eng) {
+    e = ctx->eng->upload(ctx->model);
+    if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+    e = ctx->lsqr->set_geometry(ctx->model);
+    if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
+  }
+  ctx->has_model = true;
   return FMT2D_OK;
 }
 
@@ -319,6 +352,17 @@ int fmt2d_gtg_diag(fmt2d_ctx* ctx, double* gtg) {
   return FMT2D_OK;
 }
 
+int fmt2d_set_smoothing(fmt2d_ctx* ctx, double corr_x, double corr_z, double corr_x_iface,
+                        const double* mvscale) {
+  if (!ctx || !mvscale) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const std::string e = ctx->lsqr->set_smoothing(ctx->model, corr_x, corr_z, corr_x_iface, mvscale);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  return FMT2D_OK;
+}
+
 int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residual,
                const double* gtg_diag, const double* dm_sum, double* dm, int* iters, double* rnorm,
                double* bnorm, double* test2) {
@@ -327,7 +371,8 @@ int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residua
   if (!ctx->need_gpu(code)) return code;
   if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
   if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
-  if (p->smooth_type != 1) return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1 (Laplacian)");
+  if (p->smooth_type < 1 || p->smooth_type > 3)
+    return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1, 2 or 3");
   if (p->max_iter < 1) return ctx->fail(FMT2D_ERR_ARG, "max_iter must be >= 1");
   if (ctx->lsqr->nparm() != ctx->model.n_inv_parms)
     return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the model's inversion parameters");

@@ -28,6 +28,7 @@
 // FP64 restatement's.
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include "eik64.cuh"
 #include "eik_eval.cuh"
 #include "model.h"
@@ -39,7 +40,10 @@ namespace {
 using namespace ev;
 
 // ---------------------------------------------------------------- field solve
-constexpr int kSolveThreads = 512;
+#ifndef FMT2D_SOLVE_THREADS
+#define FMT2D_SOLVE_THREADS 512
+#endif
+constexpr int kSolveThreads = FMT2D_SOLVE_THREADS;   // threads of a field's solve block
 constexpr int kSolveWarps = kSolveThreads / 32;
 constexpr int kHalfWarps = kSolveThreads / 16;
 constexpr unsigned kLCap = 4096;          // entries of each list held in shared memory
@@ -691,11 +695,34 @@ static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* t
 }
 int e64_tiles(const Fld64& f) { return tiles_of(f); }
 int e64_tiles_max() { return kTilesMax; }
+// k_solve may use up to kSmemMax of dynamic shared memory.  The attribute is
+// set once per device: changing a kernel's attributes while it runs (a solve
+// of another stage chain on another stream) waits for that kernel to finish,
+// which would serialise the chains.
+static void solve_attr_once() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  // the opt-in limit covers static and dynamic shared memory together
+  int optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k_solve) != cudaSuccess)
+    return;
+  const int dyn = std::min<int>((int)kSmemMax, optin - (int)fa.sharedSizeBytes);
+  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ==
+      cudaSuccess)
+    done[dev] = true;
+}
 void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
                unsigned long long* ctr, cudaStream_t st) {
   int smem_bits = 0, cap = 0;
   const size_t bytes = solve_smem(max_slots, max_tiles, &smem_bits, &cap);
-  cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  solve_attr_once();
   k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, cap, max_steps, ctr);
 }
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st) {

@@ -70,6 +70,44 @@ std::string put_raw(DevBuf& b, const T* v, size_t n, cudaStream_t st) {
   return std::string();
 }
 
+// Pinned staging of a lane: make room for n bytes (the lane's stream must be
+// idle: the old area may be freed), then hand out 256-byte aligned pieces.
+std::string lane_reserve(SolveLane& L, size_t n) {
+  L.pin_used = 0;
+  if (n <= L.pin_cap && L.pin) return std::string();
+  if (L.pin) cudaFreeHost(L.pin);
+  L.pin = nullptr;
+  L.pin_cap = 0;
+  const size_t cap = std::max<size_t>(n, 1 << 16);
+  if (cudaMallocHost(&L.pin, cap) != cudaSuccess) {
+    L.pin = nullptr;
+    return "pinned host allocation failed";
+  }
+  L.pin_cap = cap;
+  return std::string();
+}
+
+void* lane_take(SolveLane& L, size_t n) {
+  const size_t a = (L.pin_used + 255) / 256 * 256;
+  if (a + n > L.pin_cap) return nullptr;
+  L.pin_used = a + n;
+  return L.pin + a;
+}
+
+// put() through the lane's pinned staging (the copy is stream-ordered; the
+// staging piece is not reused before the lane's stream is idle again).
+template <class T>
+std::string put_lane(SolveLane& L, DevBuf& b, const std::vector<T>& v) {
+  b.alloc(v.size() * sizeof(T));
+  if (!b.p) return "device allocation failed";
+  if (v.empty()) return std::string();
+  void* h = lane_take(L, v.size() * sizeof(T));
+  if (!h) return "pinned staging too small";
+  std::memcpy(h, v.data(), v.size() * sizeof(T));
+  CK(cudaMemcpyAsync(b.p, h, v.size() * sizeof(T), cudaMemcpyHostToDevice, L.st));
+  return std::string();
+}
+
 // invert2d_main.f90:906-931: depth of the seafloor interface under x.
 double seafloor_at(const Model& m, double px) {
   const std::vector<double>& z = m.ifc[2].z;
@@ -333,6 +371,12 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     max_slots = std::max(max_slots, D.nslots);
   }
   if (max_slots >= (1ull << 30)) return "region too large for the eikonal solver (2^30 slots)";
+  {
+    // the lane's stream is idle here (the previous level ended with a sync)
+    const size_t per = sizeof(Fld64) + sizeof(Seed64) + 4 * sizeof(double) + 8 * sizeof(unsigned);
+    std::string e0s = lane_reserve(L, (size_t)nf * per + kCtrN * 8 + 16 * 256);
+    if (!e0s.empty()) return e0s;
+  }
   // solver scratch of the batch, per slot: staged time, gradient and flags,
   // pending time, start list, list and commit overflow, listed bitset
   const size_t words = (total + 31 * (size_t)nf + 31) / 32 + (size_t)nf;
@@ -381,9 +425,9 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     if (tf == 5) hw.push_back(i);
   }
   std::string e;
-  if (!(e = put(L.fields, hf, L.st)).empty()) return e;
-  if (!(e = put(L.up, up, L.st)).empty()) return e;
-  if (!(e = put(L.step, wstep, L.st)).empty()) return e;
+  if (!(e = put_lane(L, L.fields, hf)).empty()) return e;
+  if (!(e = put_lane(L, L.up, up)).empty()) return e;
+  if (!(e = put_lane(L, L.step, wstep)).empty()) return e;
   unsigned long long* dctr = L.ctr.as<unsigned long long>();
   CK(cudaMemsetAsync(L.sinq.p, 0, words * sizeof(unsigned), L.st));
   CK(cudaMemsetAsync(L.scnt.p, 0, (size_t)nf * 4 * sizeof(unsigned), L.st));
@@ -396,8 +440,8 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   if (level == 0) {
     std::vector<double> sx(nf), sz(nf);
     for (int i = 0; i < nf; ++i) { sx[i] = src_x_[items[i].first]; sz[i] = src_z_[items[i].first]; }
-    if (!(e = put(L.sx, sx, L.st)).empty()) return e;
-    if (!(e = put(L.sz, sz, L.st)).empty()) return e;
+    if (!(e = put_lane(L, L.sx, sx)).empty()) return e;
+    if (!(e = put_lane(L, L.sz, sz)).empty()) return e;
     e64_init_source(dF, L.sx.as<double>(), L.sz.as<double>(), nf, L.st);
     ++L.stats.launches;
   } else {
@@ -422,7 +466,7 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
       d.reflect = I.reflect;
       d.target_side = I.target_side;
     }
-    if (!(e = put(L.seeds, sd, L.st)).empty()) return e;
+    if (!(e = put_lane(L, L.seeds, sd)).empty()) return e;
     e64_seed_iface(dF, L.seeds.as<Seed64>(), nf, m_.nx, L.st);
     ++L.stats.launches;
   }
@@ -437,7 +481,10 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     return "cudaEventCreate failed";
   }
   std::string err;
-  std::vector<unsigned> hc((size_t)nf * 4);
+  unsigned* hc = static_cast<unsigned*>(lane_take(L, (size_t)nf * 4 * sizeof(unsigned)));
+  unsigned long long* hctr =
+      static_cast<unsigned long long*>(lane_take(L, kCtrN * sizeof(unsigned long long)));
+  if (!hc || !hctr) return "pinned staging too small";
   cudaEventRecord(e0, L.st);
   unsigned long long bad = 0;
   for (int pass = 0;; ++pass) {
@@ -447,7 +494,7 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     cudaMemsetAsync(L.sinq.p, 0, words * sizeof(unsigned), L.st);
     e64_verify(dF, nf, max_slots, L.st);
     ++L.stats.launches;
-    cudaError_t ce = cudaMemcpyAsync(hc.data(), L.scnt.p, hc.size() * sizeof(unsigned),
+    cudaError_t ce = cudaMemcpyAsync(hc, L.scnt.p, (size_t)nf * 4 * sizeof(unsigned),
                                      cudaMemcpyDeviceToHost, L.st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(L.st);
     if (ce != cudaSuccess) { err = std::string("eikonal solve: ") + cudaGetErrorString(ce); break; }
@@ -474,8 +521,9 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   if (!err.empty()) return err;
   L.stats.round_ms += ms;
   {
-    unsigned long long c[kCtrN];
-    CK(cudaMemcpy(c, dctr, sizeof(c), cudaMemcpyDeviceToHost));
+    unsigned long long* c = hctr;
+    CK(cudaMemcpyAsync(c, dctr, kCtrN * sizeof(unsigned long long), cudaMemcpyDeviceToHost, L.st));
+    CK(cudaStreamSynchronize(L.st));
     L.stats.evals += c[kCtrEval];
     L.stats.writes += c[kCtrWrite];
     L.stats.passed += c[kCtrPass];
@@ -495,7 +543,7 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   L.stats.launches += 2;
   CK(cudaGetLastError());
   if (!hw.empty()) {
-    if (!(e = put(L.which, hw, L.st)).empty()) return e;
+    if (!(e = put_lane(L, L.which, hw)).empty()) return e;
     L.hw.alloc(hw.size() * (size_t)m_.nx * sizeof(double));
     const double dx_if = m_.xpos[1] - m_.xpos[0];
     e64_headwave(dF, hw_slot_.as<int>(), hw_v_.as<double>(), dx_if, m_.nx,

@@ -92,10 +92,19 @@ struct SolveLane {
   DevBuf sTn, sGn, sfln, spend, sclaim, slist, sover, sinq, scnt;
   SolveStats stats;
   bool not_converged = false;
+  // pinned staging of the lane's small host <-> device copies (descriptors,
+  // counters): a pageable copy goes through the driver's shared staging
+  // path, where a read-back waiting for one chain's solve holds up the other
+  // chains' uploads and so serialises the chains
+  char* pin = nullptr;
+  size_t pin_cap = 0, pin_used = 0;
   void free_all() {
     for (DevBuf* b : {&fields, &up, &step, &sx, &sz, &seeds, &which, &hw, &ctr, &sTn, &sGn, &sfln,
                       &spend, &sclaim, &slist, &sover, &sinq, &scnt})
       b->free_();
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_cap = pin_used = 0;
   }
 };
 

@@ -128,21 +128,9 @@ __device__ __forceinline__ double warp_dot(const int* __restrict__ idx,
   return warp_sum(a0 + a1);
 }
 
-__global__ void __launch_bounds__(kLsThreads) k_ls_init_u(LsqrDev d) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  double ss = 0.0;
-  for (int i = tid; i < d.nd; i += nth) {
-    const double r = d.residual[i];
-    d.u[i] = r;
-    ss += r * r;
-  }
-  for (int j = tid; j < d.np; j += nth) {
-    const double s = -(w_smooth(d, j) * lap_at(d, d.dm_sum, j));
-    const double t = -(w_damp(d, j) * d.dm_sum[j]);
-    d.u[d.nd + j] = s;
-    d.u[d.nd + d.np + j] = t;
-    ss += s * s + t * t;
-  }
+// The right-hand side's norm (every block passes its partial sum of squares):
+// beta, and the early exit of a zero right-hand side.
+__device__ void init_u_tail(const LsqrDev& d, double ss) {
   double tot = 0.0;
   if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
     LsqrScalars& S = *d.sc;
@@ -163,31 +151,9 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_init_u(LsqrDev d) {
   }
 }
 
-// v <- A^T u (- beta v), masked; then the rotation of one LSQR step.
-__global__ void __launch_bounds__(kLsThreads) k_ls_adj(LsqrDev d) {
-  const int state = d.sc->state;
-  if (state != kLsInit && state != kLsRun) return;
-  const bool init = state == kLsInit;
-  const double beta = d.sc->beta, alpha = d.sc->alpha;
-  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarp = (gridDim.x * blockDim.x) >> 5;
-  const double* uL = d.u + d.nd;
-  const double* uD = d.u + d.nd + d.np;
-  double ss = 0.0;
-  for (int j = warp; j < d.np; j += nwarp) {
-    const double g = warp_dot(d.crow, d.cval, d.cp[j], d.cp[j + 1], d.u, d.nd);
-    if (lane == 0) {
-      double atu = g / bsc;
-      atu = atu + (w_smooth(d, j) * lap_at(d, uL, j)) / bsc;
-      atu = atu + (w_damp(d, j) * uD[j]) / bsc;
-      double vn = init ? atu : atu - beta * (d.v[j] / asc);
-      if (masked(d, j)) vn = 0.0;
-      d.v[j] = vn;
-      ss += vn * vn;
-    }
-  }
+// v's norm alpha, then either the start of the iteration (after the first
+// A^T u) or the rotation of one LSQR step.
+__device__ void adj_tail(const LsqrDev& d, double ss, bool init) {
   double tot = 0.0;
   if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
     LsqrScalars& S = *d.sc;
@@ -236,6 +202,80 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_adj(LsqrDev d) {
   }
 }
 
+// u's norm beta; the pending w / dm update is done.
+__device__ void fwd_tail(const LsqrDev& d, double ss, bool run, int state) {
+  double tot = 0.0;
+  if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
+    LsqrScalars& S = *d.sc;
+    if (run) S.beta = sqrt(tot);
+    S.pending = kPendNone;
+    if (state == kLsFinal) S.state = kLsDone;
+  }
+}
+
+// The pending w / dm update of the previous step at parameter j (vn: v_j
+// normalised).
+__device__ __forceinline__ void w_dm_update(const LsqrDev& d, int j, double vn, int pending,
+                                            double t_r, double p_r) {
+  if (pending == kPendInitW) {
+    d.w[j] = vn;
+  } else if (pending == kPendUpdate) {
+    const bool m = masked(d, j);
+    const double wo = d.w[j];
+    const double z = m ? 0.0 : wo;
+    double wn = vn - t_r * wo;
+    if (m) wn = 0.0;
+    d.w[j] = wn;
+    d.dm[j] = d.dm[j] + p_r * z;
+  }
+}
+
+__global__ void __launch_bounds__(kLsThreads) k_ls_init_u(LsqrDev d) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  double ss = 0.0;
+  for (int i = tid; i < d.nd; i += nth) {
+    const double r = d.residual[i];
+    d.u[i] = r;
+    ss += r * r;
+  }
+  for (int j = tid; j < d.np; j += nth) {
+    const double s = -(w_smooth(d, j) * lap_at(d, d.dm_sum, j));
+    const double t = -(w_damp(d, j) * d.dm_sum[j]);
+    d.u[d.nd + j] = s;
+    d.u[d.nd + d.np + j] = t;
+    ss += s * s + t * t;
+  }
+  init_u_tail(d, ss);
+}
+
+// v <- A^T u (- beta v), masked; then the rotation of one LSQR step.
+__global__ void __launch_bounds__(kLsThreads) k_ls_adj(LsqrDev d) {
+  const int state = d.sc->state;
+  if (state != kLsInit && state != kLsRun) return;
+  const bool init = state == kLsInit;
+  const double beta = d.sc->beta, alpha = d.sc->alpha;
+  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  const double* uL = d.u + d.nd;
+  const double* uD = d.u + d.nd + d.np;
+  double ss = 0.0;
+  for (int j = warp; j < d.np; j += nwarp) {
+    const double g = warp_dot(d.crow, d.cval, d.cp[j], d.cp[j + 1], d.u, d.nd);
+    if (lane == 0) {
+      double atu = g / bsc;
+      atu = atu + (w_smooth(d, j) * lap_at(d, uL, j)) / bsc;
+      atu = atu + (w_damp(d, j) * uD[j]) / bsc;
+      double vn = init ? atu : atu - beta * (d.v[j] / asc);
+      if (masked(d, j)) vn = 0.0;
+      d.v[j] = vn;
+      ss += vn * vn;
+    }
+  }
+  adj_tail(d, ss, init);
+}
+
 // u <- A v - alpha u, and the pending w / dm update of the previous step.
 __global__ void __launch_bounds__(kLsThreads) k_ls_fwd(LsqrDev d) {
   const int state = d.sc->state;
@@ -271,25 +311,188 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_fwd(LsqrDev d) {
       uD[j] = t;
       ss += s * s + t * t;
     }
-    if (pending == kPendInitW) {
-      d.w[j] = vn;
-    } else if (pending == kPendUpdate) {
-      const bool m = masked(d, j);
-      const double wo = d.w[j];
-      const double z = m ? 0.0 : wo;
-      double wn = vn - t_r * wo;
-      if (m) wn = 0.0;
-      d.w[j] = wn;
-      d.dm[j] = d.dm[j] + p_r * z;
+    w_dm_update(d, j, vn, pending, t_r, p_r);
+  }
+  fwd_tail(d, ss, run, state);
+}
+
+// ---------------------------------------------------------------- Gaussian layouts
+// smooth_type 2: u = [data | w_s R_h | w_s R_v | damping], the interface rows
+// of the R_h block holding w_si R_i instead; adjoint R_h^T, R_v^T, R_i.
+// smooth_type 3: u = [data | w_s L (velocity rows), w_si R_i (interface
+// rows) | damping]; adjoint L and R_i.  Masked velocity rows are zero in
+// every block (inversion2d.f90:6608-6736, 6753-6851, 6883-7120).
+
+// Row j of A times x, warp-cooperative (every lane gets the sum).
+__device__ __forceinline__ double row_dot(const SpRows& A, int j, const double* x, int np) {
+  if (!A.rp) return 0.0;
+  return warp_dot(A.col, A.val, A.rp[j], A.rp[j + 1], x, np);
+}
+
+__device__ __forceinline__ double* damp_block(const LsqrDev& d) {
+  return d.u + d.nd + (d.stype == 2 ? 2 : 1) * (size_t)d.np;
+}
+
+// Rows j of the smoothing blocks applied to x (unweighted by a scale):
+// s1 (the first block), s2 (the R_v block of smooth_type 2).  Warp-uniform j.
+__device__ __forceinline__ void smooth_rows(const LsqrDev& d, const double* x, int j, double* s1,
+                                            double* s2) {
+  *s2 = 0.0;
+  if (d.stype == 3) {
+    if (j < d.nvp) {
+      *s1 = w_smooth(d, j) * lap_at(d, x, j);
+    } else {
+      const double h = row_dot(d.ri, j, x, d.np);
+      *s1 = d.ws_i > 0.0 ? d.ws_i * h : 0.0;
+    }
+    return;
+  }
+  const double h = row_dot(d.rh, j, x, d.np), v = row_dot(d.rv, j, x, d.np);
+  if (j < d.nvp) {
+    const bool m = d.mask[j];
+    *s1 = d.ws_v * (m ? 0.0 : h);
+    *s2 = d.ws_v * (m ? 0.0 : v);
+  } else {
+    const bool ri = d.ws_i > 0.0 && d.ri.rp;
+    const double hi = ri ? row_dot(d.ri, j, x, d.np) : 0.0;
+    *s1 = ri ? d.ws_i * hi : 0.0;
+    *s2 = d.ws_v * v;
+  }
+}
+
+__global__ void __launch_bounds__(kLsThreads) k_ls_init_u_g(LsqrDev d) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, warp = tid >> 5, nwarp = nth >> 5;
+  double ss = 0.0;
+  for (int i = tid; i < d.nd; i += nth) {
+    const double r = d.residual[i];
+    d.u[i] = r;
+    ss += r * r;
+  }
+  double* u1 = d.u + d.nd;
+  double* u2 = u1 + d.np;
+  for (int j = warp; j < d.np; j += nwarp) {
+    double s1, s2;
+    smooth_rows(d, d.dm_sum, j, &s1, &s2);
+    if (lane == 0) {
+      u1[j] = -s1;
+      ss += s1 * s1;
+      if (d.stype == 2) {
+        u2[j] = -s2;
+        ss += s2 * s2;
+      }
     }
   }
-  double tot = 0.0;
-  if (last_block_total(d, ss, &tot) && threadIdx.x == 0) {
-    LsqrScalars& S = *d.sc;
-    if (run) S.beta = sqrt(tot);
-    S.pending = kPendNone;
-    if (state == kLsFinal) S.state = kLsDone;
+  double* uD = damp_block(d);
+  for (int j = tid; j < d.np; j += nth) {
+    const double t = -(w_damp(d, j) * d.dm_sum[j]);
+    uD[j] = t;
+    ss += t * t;
   }
+  init_u_tail(d, ss);
+}
+
+__global__ void __launch_bounds__(kLsThreads) k_ls_adj_g(LsqrDev d) {
+  const int state = d.sc->state;
+  if (state != kLsInit && state != kLsRun) return;
+  const bool init = state == kLsInit;
+  const double beta = d.sc->beta, alpha = d.sc->alpha;
+  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  const double* u1 = d.u + d.nd;
+  const double* u2 = u1 + d.np;
+  const double* uD = damp_block(d);
+  double ss = 0.0;
+  for (int j = warp; j < d.np; j += nwarp) {
+    const double g = warp_dot(d.crow, d.cval, d.cp[j], d.cp[j + 1], d.u, d.nd);
+    double a1, a2 = 0.0, ai = 0.0;
+    bool has_i = false;
+    if (d.stype == 3) {
+      if (j < d.nvp) {
+        a1 = w_smooth(d, j) * lap_at(d, u1, j);
+      } else {
+        const double h = row_dot(d.ri, j, u1, d.np);
+        a1 = d.ws_i > 0.0 ? d.ws_i * h : 0.0;
+      }
+    } else {
+      const double h = row_dot(d.rht, j, u1, d.np), v = row_dot(d.rvt, j, u2, d.np);
+      const bool m = masked(d, j);
+      a1 = d.ws_v * (m ? 0.0 : h);
+      a2 = d.ws_v * (m ? 0.0 : v);
+      if (j >= d.nvp && d.ws_i > 0.0 && d.ri.rp) {
+        ai = d.ws_i * row_dot(d.ri, j, u1, d.np);
+        has_i = true;
+      }
+    }
+    if (lane == 0) {
+      double atu = g / bsc;
+      atu = atu + a1 / bsc;
+      if (d.stype == 2) {
+        atu = atu + a2 / bsc;
+        if (has_i) atu = atu + ai / bsc;
+      }
+      atu = atu + (w_damp(d, j) * uD[j]) / bsc;
+      double vn = init ? atu : atu - beta * (d.v[j] / asc);
+      if (masked(d, j)) vn = 0.0;
+      d.v[j] = vn;
+      ss += vn * vn;
+    }
+  }
+  adj_tail(d, ss, init);
+}
+
+__global__ void __launch_bounds__(kLsThreads) k_ls_fwd_g(LsqrDev d) {
+  const int state = d.sc->state;
+  if (state != kLsRun && state != kLsFinal) return;
+  const bool run = state == kLsRun;
+  const int pending = d.sc->pending;
+  const double alpha = d.sc->alpha, beta = d.sc->beta;
+  const double t_r = d.sc->t_r, p_r = d.sc->p_r;
+  const double bsc = beta > 0.0 ? beta : 1.0, asc = alpha > 0.0 ? alpha : 1.0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  double ss = 0.0;
+  double* u1 = d.u + d.nd;
+  double* u2 = u1 + d.np;
+  double* uD = damp_block(d);
+  if (run) {
+    for (int i = warp; i < d.nd; i += nwarp) {
+      const double g = warp_dot(d.col, d.val, d.rp[i], d.rp[i + 1], d.v, d.np);
+      if (lane == 0) {
+        const double un = g / asc - alpha * (d.u[i] / bsc);
+        d.u[i] = un;
+        ss += un * un;
+      }
+    }
+    for (int j = warp; j < d.np; j += nwarp) {
+      double s1, s2;
+      smooth_rows(d, d.v, j, &s1, &s2);
+      if (lane == 0) {
+        const double a = s1 / asc - alpha * (u1[j] / bsc);
+        u1[j] = a;
+        ss += a * a;
+        if (d.stype == 2) {
+          const double b = s2 / asc - alpha * (u2[j] / bsc);
+          u2[j] = b;
+          ss += b * b;
+        }
+      }
+    }
+  }
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int j = tid; j < d.np; j += nth) {
+    const double vn = d.v[j] / asc;
+    if (run) {
+      const double t = w_damp(d, j) * vn - alpha * (uD[j] / bsc);
+      uD[j] = t;
+      ss += t * t;
+    }
+    w_dm_update(d, j, vn, pending, t_r, p_r);
+  }
+  fwd_tail(d, ss, run, state);
 }
 
 __global__ void k_spmv_rows(LsqrDev d, const double* __restrict__ x, double* __restrict__ y) {
@@ -375,13 +578,16 @@ __global__ void k_csc_fill(const int* perm, const int* row_of, const double* val
 }  // namespace
 
 void lsqr_launch_init_u(const LsqrDev& d, int grid, cudaStream_t st) {
-  k_ls_init_u<<<grid, kLsThreads, 0, st>>>(d);
+  if (d.stype == 1) k_ls_init_u<<<grid, kLsThreads, 0, st>>>(d);
+  else k_ls_init_u_g<<<grid, kLsThreads, 0, st>>>(d);
 }
 void lsqr_launch_adj(const LsqrDev& d, int grid, cudaStream_t st) {
-  k_ls_adj<<<grid, kLsThreads, 0, st>>>(d);
+  if (d.stype == 1) k_ls_adj<<<grid, kLsThreads, 0, st>>>(d);
+  else k_ls_adj_g<<<grid, kLsThreads, 0, st>>>(d);
 }
 void lsqr_launch_fwd(const LsqrDev& d, int grid, cudaStream_t st) {
-  k_ls_fwd<<<grid, kLsThreads, 0, st>>>(d);
+  if (d.stype == 1) k_ls_fwd<<<grid, kLsThreads, 0, st>>>(d);
+  else k_ls_fwd_g<<<grid, kLsThreads, 0, st>>>(d);
 }
 void lsqr_launch_spmv(const LsqrDev& d, int transpose, const double* x, double* y, int grid,
                       cudaStream_t st) {
@@ -413,6 +619,9 @@ Lsqr::~Lsqr() {
 
 std::string Lsqr::set_geometry(const Model& m) {
   const int nx = m.nx, nz = m.nz;
+  // a new model: the smoothing matrices of the last one no longer apply
+  for (bool& h : have_sm_) h = false;
+  sm_np_ = -1;
   nvp_ = m.n_vel_parms;
   if_start_ = m.n_vel_parms;
   if_n_ = m.iface_inv > 0 ? nx : 0;
@@ -562,16 +771,90 @@ std::string Lsqr::gtg_diag(double* out) {
   return std::string();
 }
 
+namespace {
+
+// 1-based host CSR (np rows) -> 0-based device CSR; with transpose, the CSR of
+// the transpose (entries of a row of A^T in ascending row order of A).
+std::string upload_csr(const std::vector<int>& rp1, const std::vector<int>& col1,
+                       const std::vector<double>& val, bool transpose, int np, DevBuf& rp_d,
+                       DevBuf& col_d, DevBuf& val_d, cudaStream_t st) {
+  const size_t nnz = col1.size();
+  std::vector<int> rp(np + 1, 0), col(nnz);
+  std::vector<double> v(nnz);
+  if (!transpose) {
+    for (int i = 0; i <= np; ++i) rp[i] = rp1[i] - 1;
+    for (size_t k = 0; k < nnz; ++k) col[k] = col1[k] - 1;
+    v = val;
+  } else {
+    for (size_t k = 0; k < nnz; ++k) ++rp[col1[k]];   // counts at (col - 1) + 1
+    for (int i = 0; i < np; ++i) rp[i + 1] += rp[i];
+    std::vector<int> next(rp.begin(), rp.end() - 1);
+    for (int i = 0; i < np; ++i)
+      for (int k = rp1[i] - 1; k < rp1[i + 1] - 1; ++k) {
+        const int q = next[col1[k] - 1]++;
+        col[q] = i;
+        v[q] = val[k];
+      }
+  }
+  rp_d.alloc((size_t)(np + 1) * 4);
+  col_d.alloc(std::max<size_t>(nnz, 1) * 4);
+  val_d.alloc(std::max<size_t>(nnz, 1) * 8);
+  if (!rp_d.p || !col_d.p || !val_d.p) return "device allocation failed (smoothing matrix)";
+  LCK(cudaMemcpyAsync(rp_d.p, rp.data(), (size_t)(np + 1) * 4, cudaMemcpyHostToDevice, st));
+  if (nnz) {
+    LCK(cudaMemcpyAsync(col_d.p, col.data(), nnz * 4, cudaMemcpyHostToDevice, st));
+    LCK(cudaMemcpyAsync(val_d.p, v.data(), nnz * 8, cudaMemcpyHostToDevice, st));
+  }
+  LCK(cudaStreamSynchronize(st));
+  return std::string();
+}
+
+}  // namespace
+
+std::string Lsqr::set_smoothing(const Model& m, double corr_x, double corr_z, double corr_x_iface,
+                                const double* mvscale) {
+  if (!mvscale) return "null mvscale";
+  cudaSetDevice(device_);
+  const int np = m.n_inv_parms;
+  for (bool& h : have_sm_) h = false;
+  sm_np_ = np;
+  std::vector<int> rp, col;
+  std::vector<double> val;
+  // R_h -> slots 0 (R_h) and 1 (R_h^T), R_v -> 2 and 3, interface R_h -> 4
+  const struct { int which; double c; int slot; } mats[3] = {
+      {0, corr_x, 0}, {1, corr_z, 2}, {2, corr_x_iface, 4}};
+  for (const auto& q : mats) {
+    if (!(q.c > 0.0)) continue;
+    if (q.which == 2 && m.iface_inv <= 0) continue;
+    std::string e = gauss_smooth_csr(m, q.which, corr_x, corr_z, corr_x_iface, mvscale, rp, col, val);
+    if (!e.empty()) return e;
+    e = upload_csr(rp, col, val, false, np, sm_rp_[q.slot], sm_col_[q.slot], sm_val_[q.slot], st_);
+    if (!e.empty()) return e;
+    have_sm_[q.slot] = true;
+    if (q.which < 2) {
+      e = upload_csr(rp, col, val, true, np, sm_rp_[q.slot + 1], sm_col_[q.slot + 1],
+                     sm_val_[q.slot + 1], st_);
+      if (!e.empty()) return e;
+      have_sm_[q.slot + 1] = true;
+    }
+  }
+  return std::string();
+}
+
 std::string Lsqr::solve(const LsqrParams& p, const double* residual, const double* gtg,
                         const double* dm_sum, double* dm, LsqrOut* out) {
   if (!rp_.p) return "no matrix set";
   if (!have_geom_) return "no model geometry for the smoothing operator";
-  if (p.smooth_type != 1) return "smooth_type must be 1 (Laplacian)";
+  if (p.smooth_type < 1 || p.smooth_type > 3) return "smooth_type must be 1, 2 or 3";
   if (p.max_iter < 1) return "max_iter must be >= 1";
   if (np_ != if_start_ + if_n_) return "matrix columns differ from the model's inversion parameters";
   if (!dm) return "null output";
+  if (p.smooth_type != 1 && sm_np_ != np_)
+    return "smooth_type 2 and 3 need the Gaussian matrices of this model (set_smoothing)";
+  if (p.smooth_type == 2 && p.w_smooth > 0.0 && !(have_sm_[0] && have_sm_[2]))
+    return "smooth_type 2 with w_smooth > 0 needs R_h and R_v (corr_x, corr_z > 0)";
   cudaSetDevice(device_);
-  const size_t na = (size_t)nd_ + 2 * (size_t)np_;
+  const size_t na = (size_t)nd_ + (p.smooth_type == 2 ? 3 : 2) * (size_t)np_;
   res_.alloc((size_t)std::max(nd_, 1) * 8);
   dms_.alloc((size_t)np_ * 8);
   gtg_.alloc((size_t)np_ * 8);
@@ -608,6 +891,23 @@ std::string Lsqr::solve(const LsqrParams& p, const double* residual, const doubl
   d.wd_v = p.wdv;
   d.wd_i = p.wdv_iface;
   d.max_iter = p.max_iter;
+  d.stype = p.smooth_type;
+  if (d.stype != 1) {
+    auto rows = [&](int k) {
+      SpRows r;
+      if (have_sm_[k]) {
+        r.rp = sm_rp_[k].as<int>();
+        r.col = sm_col_[k].as<int>();
+        r.val = sm_val_[k].as<double>();
+      }
+      return r;
+    };
+    d.rh = rows(0);
+    d.rht = rows(1);
+    d.rv = rows(2);
+    d.rvt = rows(3);
+    d.ri = rows(4);
+  }
   int launches = 0;
   if (gtg) {
     LCK(cudaMemcpyAsync(gtg_.p, gtg, (size_t)np_ * 8, cudaMemcpyHostToDevice, st_));

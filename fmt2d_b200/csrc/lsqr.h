@@ -16,7 +16,7 @@
 namespace fmt2d {
 
 struct LsqrParams {
-  int smooth_type = 1;          // 1: Laplacian (velocity + interface)
+  int smooth_type = 1;          // 1: Laplacian; 2: Gaussian R_h, R_v; 3: Laplacian + interface R_h
   double wdv = 0, wdv_iface = 0, w_smooth = 0, w_smooth_iface = 0, eps_min = 0;
   int max_iter = 2000;
 };
@@ -41,6 +41,15 @@ struct LsqrScalars {
 enum { kLsInit = 0, kLsRun = 1, kLsFinal = 2, kLsDone = 3 };
 enum { kPendNone = 0, kPendInitW = 1, kPendUpdate = 2 };
 
+// A sparse matrix over the inversion parameters (0-based CSR, np rows; rows
+// the matrix does not cover are empty).  rp == nullptr: no matrix (all rows
+// empty).
+struct SpRows {
+  const int* rp = nullptr;
+  const int* col = nullptr;
+  const double* val = nullptr;
+};
+
 // Kernel view of one solve.
 struct LsqrDev {
   int nd = 0, np = 0, nvp = 0;
@@ -54,9 +63,15 @@ struct LsqrDev {
   int if_start = 0, if_n = 0;   // inverted interface parameters [if_start, if_start+if_n)
   const uint8_t* mask = nullptr;// 1: velocity column masked (gtg < 0.01 eps_min)
   double ws_v = 0, ws_i = 0, wd_v = 0, wd_i = 0;
+  // smooth_type and, for 2 and 3, the Gaussian operators: R_h, R_v and their
+  // transposes, the interface R_h (applied as its own adjoint, as the
+  // reference does)
+  int stype = 1;
+  SpRows rh, rht, rv, rvt, ri;
   const double* residual = nullptr;
   const double* dm_sum = nullptr;
-  double* u = nullptr;          // nd + 2 np: [data | smoothing | damping], scale 1/beta
+  double* u = nullptr;          // [data | smoothing (np; 2 np for smooth_type 2) | damping],
+                                // scale 1/beta
   double* v = nullptr;          // np, scale 1/alpha
   double* w = nullptr;          // np
   double* dm = nullptr;         // np
@@ -69,6 +84,8 @@ struct LsqrDev {
 // need one fixed grid).
 constexpr int kLsThreads = 256;
 
+// smooth_type 1 uses the Laplacian kernels, 2 and 3 the general ones (same
+// scalar recurrences); the launch functions pick by d.stype.
 void lsqr_launch_init_u(const LsqrDev& d, int grid, cudaStream_t st);
 void lsqr_launch_adj(const LsqrDev& d, int grid, cudaStream_t st);
 void lsqr_launch_fwd(const LsqrDev& d, int grid, cudaStream_t st);
@@ -84,6 +101,12 @@ class Lsqr {
   ~Lsqr();
   // Laplacian neighbour table of the model's inversion numbering.
   std::string set_geometry(const Model& m);
+  // Gaussian smoothing operators of the smooth_type 2/3 layouts
+  // (build_gauss_smooth_matrix / build_iface_gauss_smooth_matrix with the
+  // column scaling mvscale folded in): R_h if corr_x > 0, R_v if corr_z > 0,
+  // the interface R_h if corr_x_iface > 0 and an interface is inverted.
+  std::string set_smoothing(const Model& m, double corr_x, double corr_z, double corr_x_iface,
+                            const double* mvscale);
   // G from a host CSR (index base 0 or 1, as read_frechet_data2d's 1-based
   // arrays).  Builds the device CSR and CSC.
   std::string set_matrix(int ndata, int nparm, const int* row_ptr, const int* col,
@@ -112,6 +135,10 @@ class Lsqr {
   int grid_ = 0;
   DevBuf rp_, col_, val_, cp_, crow_, cval_, nb_, mask_, res_, dms_, gtg_, u_, v_, w_, dm_,
       part_, sc_, x_, y_;
+  // smoothing matrices: R_h, R_h^T, R_v, R_v^T, interface R_h
+  DevBuf sm_rp_[5], sm_col_[5], sm_val_[5];
+  bool have_sm_[5] = {false, false, false, false, false};
+  int sm_np_ = -1;           // parameters the smoothing matrices were built for
   LsqrScalars* h_sc_ = nullptr;
   double last_ms_ = 0;
   int last_launches_ = 0;

@@ -263,8 +263,21 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
       m.vel[m.g(ix, iz)] = v;
     }
   }
+  m.zbot = zrel[nzs - 1] + maxtopo;
+  m.iface_inv = iface_inv;
+  build_geometry(m, topo, sed_z, moho_z);
+  return std::string();
+}
+
+// Interfaces, regions, codes and the inversion numbering from the
+// propagation-grid velocity m.vel and the seafloor, sediment-base and Moho
+// depths (invert2d_main.f90:342-477; rebuild_geometry2d,
+// inversion2d.f90:3661-3816, redoes the same after an interface update).
+void build_geometry(Model& m, const double* topo, const double* sed_z, const double* moho_z) {
+  const int nx = m.nx, nz = m.nz;
+  const double dx = m.dx;
   m.cell_cut.assign((size_t)nx * nz, 0);
-  std::vector<double> z1(nx, 0.0), z5(nx, zrel[nzs - 1] + maxtopo);
+  std::vector<double> z1(nx, 0.0), z5(nx, m.zbot);
   build_interface(m, 1, z1.data());
   build_interface(m, 2, topo);
   build_interface(m, 3, sed_z);
@@ -313,8 +326,27 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
       if (grid_z(m, iz) - zsf >= 0.0) m.inv_idx[m.g(ix, iz)] = ++np;
     }
   m.n_vel_parms = np;
-  m.iface_inv = iface_inv;
-  m.n_inv_parms = np + (iface_inv > 0 ? nx : 0);
+  m.n_inv_parms = np + (m.iface_inv > 0 ? nx : 0);
+}
+
+std::string update_model(Model& m, const double* vel, const double* iface_z) {
+  if (m.nx == 0) return "no model";
+  const size_t n = (size_t)m.nx * m.nz;
+  if (vel) {
+    for (size_t i = 0; i < n; ++i)
+      if (!(vel[i] > 0.0)) return "velocities must be positive";
+    m.vel.assign(vel, vel + n);
+  }
+  std::vector<double> z[6];
+  for (int k = 2; k <= 4; ++k) z[k] = m.ifc[k].z;
+  if (iface_z) {
+    if (m.iface_inv < 2 || m.iface_inv > 4) return "no inverted interface to update";
+    z[m.iface_inv].assign(iface_z, iface_z + m.nx);
+  }
+  const int nvp = m.n_vel_parms, npar = m.n_inv_parms;
+  build_geometry(m, z[2].data(), z[3].data(), z[4].data());
+  if (m.n_vel_parms != nvp || m.n_inv_parms != npar)
+    return "the update changed the inversion parameters";
   return std::string();
 }
 

@@ -85,6 +85,7 @@ struct Model {
   // inversion numbering (iz outer, ix inner over nodes at or below the seafloor)
   std::vector<int> inv_idx;
   int n_vel_parms = 0, n_inv_parms = 0, iface_inv = 0;
+  double zbot = 0;                          // depth of the bottom interface (5)
   size_t g(int ix, int iz) const { return (size_t)iz * nx + ix; }
 };
 
@@ -94,6 +95,16 @@ struct Model {
 std::string build_model(Model& m, int nx, int nzs, const double* xpos, const double* topo,
                         const double* zrel, const double* vel, double vwater,
                         const double* sed_z, const double* moho_z, int iface_inv);
+
+// The geometry (interfaces, regions, codes, inversion numbering) from m.vel
+// and the seafloor, sediment-base and Moho depths.
+void build_geometry(Model& m, const double* topo, const double* sed_z, const double* moho_z);
+
+// A model step (apply_model_step, src/inversion2d.f90:7173-7237, then
+// rebuild_geometry2d, :3661-3816): the propagation-grid velocity (nz x nx,
+// ix fastest; NULL keeps it) and the depths of the inverted interface's nodes
+// (NULL keeps them); the geometry is rebuilt.  Returns an error message or "".
+std::string update_model(Model& m, const double* vel, const double* iface_z);
 
 // Gaussian smoothing matrix of the smooth_type 2/3 LSQR layouts as 1-based
 // CSR over all n_inv_parms rows (rows it does not cover stay empty), mvscale

@@ -98,23 +98,34 @@ def checkerboard_model(nx: int, dx: float, zrel_max: float, nzs: int, *, n_obs: 
                       moho_z=moho, obs_x=obs_x, picks=picks, name=name)
 
 
-def config(k: int) -> SmeshModel:
+def config(k: int, cb_amp: float | None = None) -> SmeshModel:
     """The benchmark configurations (sizes of the reference experiments
-    scaled up to the 2001x401 and 4001x601 grids) and small test models."""
+    scaled up to the 2001x401 and 4001x601 grids) and small test models.
+    cb_amp overrides the checkerboard amplitude (0: the smooth model)."""
+    cb = {} if cb_amp is None else {"cb_amp": float(cb_amp)}
     if k == 0:   # 401x121 at 0.25 km, 10 OBS, 200 shots, Pg
         return checkerboard_model(401, 0.25, 21.5, 87, n_obs=10, obs_spacing=10.0,
                                   shot_spacing=0.5, lower_crust=False, seed=0,
-                                  phases=(1,), name="pg-401x121")
+                                  phases=(1,), name="pg-401x121", **cb)
     if k == 1:   # 2001x401 at 0.1 km, 30 OBS, 1000 shots, Pg + PmP
         return checkerboard_model(2001, 0.1, 31.5, 127, n_obs=30, obs_spacing=6.5,
                                   shot_spacing=0.2, lower_crust=True, seed=1,
-                                  phases=(1, 3), name="pg-pmp-2001x401")
+                                  phases=(1, 3), name="pg-pmp-2001x401", **cb)
     if k == 4:   # 4001x601 at 0.1 km, 100 OBS, 4000 shots, all phases
         return checkerboard_model(4001, 0.1, 51.5, 207, n_obs=100, obs_spacing=4.0,
                                   shot_spacing=0.1, lower_crust=True, seed=4,
                                   moho_base=18.0, moho_amp=2.0, cb_dx=20.0, cb_dz=6.0,
-                                  phases=(1, 2, 3, 4, 5), name="joint-4001x601")
+                                  phases=(1, 2, 3, 4, 5), name="joint-4001x601", **cb)
     raise ValueError(f"unknown config {k}")
+
+
+def start_model(k: int) -> SmeshModel:
+    """Starting model of the inversion benchmark on configuration k: the
+    smooth model (no checkerboard) with a flat Moho at the true Moho's mean
+    depth; the true model is config(k)."""
+    import dataclasses
+    m = config(k, cb_amp=0.0)
+    return dataclasses.replace(m, moho_z=np.full_like(m.moho_z, float(m.moho_z.mean())))
 
 
 def small_model(nx: int = 121, dx: float = 0.25, zrel_max: float = 8.0, nzs: int = 33,

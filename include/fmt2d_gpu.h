@@ -84,6 +84,21 @@ FMT2D_API int fmt2d_last_error(fmt2d_ctx* ctx, char* buf, int len);
 FMT2D_API int fmt2d_upload_model(fmt2d_ctx* ctx, const fmt2d_model_desc* desc);
 /* Grid size after the dz = dx resampling (invert2d_main.f90:242-246). */
 FMT2D_API int fmt2d_model_info(fmt2d_ctx* ctx, int* nx, int* nz, double* dx, double* x0);
+/* The propagation-grid velocity vel[nz*nx] (ix fastest) of the current model:
+ * the velocity grid the inversion updates (vgrid%velocity, inverted on the
+ * propagation grid itself). */
+FMT2D_API int fmt2d_model_velocity(fmt2d_ctx* ctx, double* vel);
+/* Depths z[nx] of interface k (1 sea surface, 2 seafloor, 3 sediment base,
+ * 4 Moho, 5 model bottom), node ix on grid column ix (intrface(k)%z_nodes). */
+FMT2D_API int fmt2d_model_interface(fmt2d_ctx* ctx, int k, double* z);
+/* A model step of the inversion: what apply_model_step leaves
+ * (src/inversion2d.f90:7173-7237) followed by rebuild_geometry2d
+ * (:3661-3816).  vel[nz*nx] is the new propagation-grid velocity (NULL keeps
+ * it), iface_z[nx] the new depths of the inverted interface (NULL keeps
+ * them).  The geometry is rebuilt on the host and uploaded; field stores stay
+ * allocated, every field is unsolved until the next forward.  The inversion
+ * numbering must not change (FMT2D_ERR_MODEL otherwise, the model unchanged). */
+FMT2D_API int fmt2d_update_model(fmt2d_ctx* ctx, const double* vel, const double* iface_z);
 /* Region r (1..6): node count and, when arrays are given, the reference's node
  * table (i1 = grid column 1-based or 0 for interface nodes, i2 = grid row
  * 1-based or interface id, i3 = interface node index 1-based or 0). */
@@ -231,9 +246,13 @@ FMT2D_API int fmt2d_spmv(fmt2d_ctx* ctx, int transpose, const double* x, double*
 /* gtg[j] = sum over rows of G(i,j)^2, j = 1..nparm. */
 FMT2D_API int fmt2d_gtg_diag(fmt2d_ctx* ctx, double* gtg);
 
-/* run_lsqr's arguments that are not arrays.  smooth_type 1 (Laplacian) is the
- * augmented system [G; w_s L; w_d I] with the model's inversion numbering;
- * max_iter is the reference's min(lsqr_max_iter, 2000), >= 1. */
+/* run_lsqr's arguments that are not arrays (src/inversion2d.f90:6578-6598).
+ * smooth_type selects the augmented system (:507-511): 1 [G; w_s L; w_d I]
+ * with the Laplacian over the model's inversion numbering; 2 [G; w_s R_h;
+ * w_s R_v; w_d I] with the interface Gaussian w_si R_i in the R_h block's
+ * interface rows; 3 [G; w_s L (velocity rows) + w_si R_i (interface rows);
+ * w_d I].  2 and 3 need fmt2d_set_smoothing first.  max_iter is the
+ * reference's min(lsqr_max_iter, 2000), >= 1. */
 typedef struct fmt2d_lsqr_params {
   int smooth_type;
   int max_iter;
@@ -241,6 +260,20 @@ typedef struct fmt2d_lsqr_params {
   double w_smooth, w_smooth_iface;  /* smoothing weights */
   double eps_min;                   /* velocity columns with gtg < 0.01 eps_min are masked */
 } fmt2d_lsqr_params;
+
+/* The Gaussian smoothing operators of smooth_type 2 and 3:
+ * build_gauss_smooth_matrix (R_h along grid rows within 3 corr_x, R_v along
+ * grid columns within 3 corr_z) and build_iface_gauss_smooth_matrix (R_i along
+ * the inverted interface within 3 corr_x_iface), src/inversion2d.f90:1252-1616,
+ * with the column scaling mvscale[nparm] folded in as the reference does.
+ * Built on the host, kept on the device (R_h and R_v also transposed) for the
+ * following fmt2d_lsqr calls until the next model upload.  R_h is built when
+ * corr_x > 0, R_v when corr_z > 0, R_i when corr_x_iface > 0 and an interface
+ * is inverted.  R_i is applied as its own adjoint, as the reference does
+ * (:6826-6833), which is its transpose when the interface columns share one
+ * scaling. */
+FMT2D_API int fmt2d_set_smoothing(fmt2d_ctx* ctx, double corr_x, double corr_z,
+                                  double corr_x_iface, const double* mvscale);
 
 /* LSQR on the current G: residual[ndata], gtg_diag[nparm] (NULL: computed
  * from G), dm_sum[nparm] (NULL: zeros) -> dm[nparm] and the reference's
