@@ -400,8 +400,13 @@ def inversion_iterations(local, n_iter: int = 2):
 def run_ours(args, world, rank, local):
     from fmt2d_b200 import synth
     from fmt2d_b200.api import fields_of, phase_mask
+    global PHASES
+    if args.phases:
+        PHASES = tuple(int(p) for p in args.phases.split(","))
     m = synth.config(1)
     src = source_set(m, rank, world)
+    if args.sources > 0:
+        src = src[:args.sources]
     mask = phase_mask(PHASES)
     cpu, checked = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -569,6 +574,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-inversion", action="store_true",
                     help="skip the s-per-inversion-iteration leg")
+    ap.add_argument("--sources", type=int, default=0,
+                    help="solve only the first N sources (profiling captures; 0: all 30)")
+    ap.add_argument("--phases", default="",
+                    help="comma-separated phase ids to solve (profiling captures; default 1,3)")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-core arm: rank 0 alone runs it, the other ranks exit without work

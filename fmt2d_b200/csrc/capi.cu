@@ -279,6 +279,16 @@ int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, doub
   return FMT2D_OK;
 }
 
+int fmt2d_get_field_device(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, double* gz) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const std::string e = ctx->eng->get_field_device(src, tf, T, gx, gz);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  return FMT2D_OK;
+}
+
 int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n) {
   if (!ctx || !values || n < 0) return FMT2D_ERR_ARG;
   int code = 0;

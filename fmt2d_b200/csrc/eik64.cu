@@ -41,7 +41,7 @@ using namespace ev;
 
 // ---------------------------------------------------------------- field solve
 #ifndef FMT2D_SOLVE_THREADS
-#define FMT2D_SOLVE_THREADS 512
+#define FMT2D_SOLVE_THREADS 384
 #endif
 constexpr int kSolveThreads = FMT2D_SOLVE_THREADS;   // threads of a field's solve block
 constexpr int kSolveWarps = kSolveThreads / 32;

@@ -560,6 +560,21 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   return std::string();
 }
 
+std::string Engine::get_field_device(int src, int tf, double* T, double* gx, double* gz) {
+  cudaSetDevice(device_);
+  if (src < 0 || src >= (int)fields_.size() || tf < 1 || tf > 12) return "bad field index";
+  const FieldStore& F = fields_[src][tf];
+  if (!F.solved) return "time field not solved";
+  const Region& G = m_.reg[kTf[tf].reg];
+  const DevRegionStore& D = reg_[kTf[tf].reg];
+  e64_export(F.T.as<double>(), F.Gout.as<double2>(), D.slot_of_node.as<int>(), G.nnode, T, gx, gz,
+             stream_);
+  ++stats_.launches;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(stream_));
+  return std::string();
+}
+
 std::string Engine::get_field(int src, int tf, double* T, double* gx, double* gz) {
   cudaSetDevice(device_);
   if (src < 0 || src >= (int)fields_.size() || tf < 1 || tf > 12) return "bad field index";

@@ -117,6 +117,8 @@ class Engine {
   // (placed on the seafloor), one slot per source.
   std::string forward(const double* sx, int nsrc, int phase_mask);
   std::string get_field(int src, int tf, double* T, double* gx, double* gz);
+  // the same into device memory of the caller (any may be null)
+  std::string get_field_device(int src, int tf, double* T, double* gx, double* gz);
   // Ray backtrace and Frechet rows of npick picks (source index, phase 1..5,
   // receiver x, z) on the fields of the last forward; the rows stay on the
   // device until frechet_rows copies them out (CSR over all picks, invalid

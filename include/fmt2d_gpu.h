@@ -194,6 +194,12 @@ FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int p
 /* Time field tf (1..12) of source s in its region's node order, FP64; any of
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
+/* fmt2d_get_field into DEVICE memory of the caller (T, dtdx, dtdz: nnode
+ * doubles each on the context's device, any may be NULL); complete when the
+ * call returns.  No reference counterpart (the reference's fields are host
+ * arrays); the PyTorch operators use it to return CUDA tensors. */
+FMT2D_API int fmt2d_get_field_device(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx,
+                                     double* dtdz);
 /* Counters of the last fmt2d_forward (and of the exports since), in this
  * order: [0] steps of the longest field solve, summed over stage levels,
  * [1] stage levels, [2] solve passes (each ends in a fixed-point check of
