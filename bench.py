@@ -397,6 +397,37 @@ def inversion_iterations(local, n_iter: int = 2):
             "note": "wall clock through the public API, 1 GPU"}
 
 
+def uneven_batch(local, n_models: int, stream_dev):
+    """The uneven multi-model batch: n_models seeded models of grid sizes from
+    401x121 to 2001x401, up to 20 OBS each, all five phases, solved in one
+    fmt2d_forward_batch call; the same models one fmt2d_forward after another
+    beside it.  Fields/s, wall clock on the device's work (the calls return
+    when their fields are solved)."""
+    from fmt2d_b200 import synth
+    from fmt2d_b200.api import Fmt2d, fields_of, forward_batch, phase_mask
+    phases = (1, 2, 3, 4, 5)
+    models = [synth.uneven_model(k, max_obs=20) for k in range(n_models)]
+    ctxs = [Fmt2d(local).upload(m) for m in models]
+    srcs = [np.asarray(m.obs_x, dtype=np.float64) for m in models]
+    nf = sum(x.size for x in srcs) * len(fields_of(phase_mask(phases)))
+    forward_batch(ctxs, srcs, phases)                       # warm (field stores)
+    t0 = time.perf_counter()
+    forward_batch(ctxs, srcs, phases)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for g, x in zip(ctxs, srcs):
+        g.forward(x, phases)
+    ts = time.perf_counter() - t0
+    sizes = [f"{m.nx}x{g.nz}" for m, g in zip(models, ctxs)]
+    for g in ctxs:
+        g.close()
+    return {"value": round(nf / tb, 3), "unit": "fields/s", "models": n_models, "fields": nf,
+            "s": round(tb, 3), "one_model_at_a_time": {"value": round(nf / ts, 3),
+                                                       "s": round(ts, 3)},
+            "grids": sizes, "phases": "all five",
+            "note": "fmt2d_forward_batch over the models' contexts vs fmt2d_forward per model"}
+
+
 def run_ours(args, world, rank, local):
     from fmt2d_b200 import synth
     from fmt2d_b200.api import fields_of, phase_mask
@@ -430,7 +461,8 @@ def run_ours(args, world, rank, local):
     g = Fmt2d(local).upload(m)
     stream = torch.cuda.ExternalStream(g.stream(), device=dev)
     nf = len(fields_of(mask)) * src.size
-    terminal = [1, 5]          # last stage of Pg and of PmP (ray tracing starts there)
+    # the last stage of each phase (ray tracing starts there)
+    terminal = sorted({{1: 1, 2: 3, 3: 5, 4: 8, 5: 12}[p] for p in PHASES})
 
     for _ in range(args.warmup):
         g.forward(src, PHASES)
@@ -516,6 +548,14 @@ def run_ours(args, world, rank, local):
         except Exception as ex:
             inversion = {"unavailable": str(ex)[:200]}
 
+    # ---- the uneven multi-model batch (outside the timed region)
+    batch = None
+    if world == 1 and args.models > 0:
+        try:
+            batch = uneven_batch(local, args.models, dev)
+        except Exception as ex:
+            batch = {"unavailable": str(ex)[:200]}
+
     # ---- the plain form, one source (its stage solves) per fmt2d_forward call,
     # on a few sources: the denominator of "batched vs plain"
     try:
@@ -557,7 +597,7 @@ def run_ours(args, world, rank, local):
                         "bytes_per_node": 16, "fp64_bytes_per_node": 36,
                         "fp64_frac": round(36.0 * nodes_step / (step_ms / 1e3) / 1e9 / peak, 7)},
            "solver": solver,
-           "rays": rays, "lsqr": lsqr, "inversion": inversion,
+           "rays": rays, "lsqr": lsqr, "inversion": inversion, "uneven_batch": batch,
            "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "cpu_baseline": cpu}
@@ -574,6 +614,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-inversion", action="store_true",
                     help="skip the s-per-inversion-iteration leg")
+    ap.add_argument("--models", type=int, default=8,
+                    help="models of the uneven multi-model batch leg (0: skip)")
     ap.add_argument("--sources", type=int, default=0,
                     help="solve only the first N sources (profiling captures; 0: all 30)")
     ap.add_argument("--phases", default="",

@@ -62,6 +62,29 @@ def select_data(phase, obs, t_calc, valid, row_ptr, gindx, gval, mvscale, *, cri
     return rp[:k + 1], gi[:kk], gv[:kk], res[:k], wt[:k], pk[:k]
 
 
+def forward_batch(contexts, sources, phases=(1, 2, 3, 4, 5)):
+    """fmt2d_forward of several contexts (one model each) at once: contexts
+    is a list of Fmt2d, sources a list of OBS x arrays (one per context);
+    phases applies to all.  Raises on the first failing context."""
+    n = len(contexts)
+    if n == 0 or len(sources) != n:
+        raise ValueError("one source array per context")
+    xs = [np.ascontiguousarray(x, dtype=np.float64) for x in sources]
+    hs = (C.c_void_p * n)(*[g.h.value for g in contexts])
+    ps = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+    ns = np.array([x.size for x in xs], dtype=np.int32)
+    mask = phase_mask(phases)
+    ms = np.full(n, mask, dtype=np.int32)
+    st = np.zeros(n, dtype=np.int32)
+    rc = N.lib().fmt2d_forward_batch(hs, n, ps, N.ptr(ns), N.ptr(ms), N.ptr(st))
+    for g, x in zip(contexts, xs):
+        g.mask, g.nsrc = mask, x.size
+    if rc != 0:
+        i = int(np.flatnonzero(st != 0)[0])
+        contexts[i]._check(int(st[i]), f"fmt2d_forward_batch (context {i})")
+    return contexts
+
+
 def project_rows(row_ptr, gindx, gval, nfine, p_row_ptr, p_col, p_val):
     """Rows of G P (fmt2d_project_rows): 1-based CSR (row_ptr, gindx, gval)
     over the fine parameters mapped onto a coarse grid's parameters."""

@@ -7,6 +7,8 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
+#include <vector>
 
 struct fmt2d_ctx {
   std::unique_ptr<fmt2d::Engine> eng;   // null for a host-only context
@@ -267,6 +269,27 @@ int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask)
   if (!e.empty())
     return ctx->fail(ctx->eng->not_converged() ? FMT2D_ERR_CONVERGE : FMT2D_ERR_CUDA, e);
   return FMT2D_OK;
+}
+
+int fmt2d_forward_batch(fmt2d_ctx* const* ctxs, int n, const double* const* src_x,
+                        const int* nsrc, const int* phase_mask, int* status) {
+  if (!ctxs || n <= 0 || !src_x || !nsrc || !phase_mask) return FMT2D_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j)
+      if (ctxs[i] == ctxs[j]) return FMT2D_ERR_ARG;   // one forward per context
+  std::vector<int> rc(n, FMT2D_OK);
+  auto run = [&](int i) { rc[i] = fmt2d_forward(ctxs[i], src_x[i], nsrc[i], phase_mask[i]); };
+  std::vector<std::thread> th;
+  th.reserve(n > 1 ? n - 1 : 0);
+  for (int i = 1; i < n; ++i) th.emplace_back(run, i);
+  run(0);
+  for (std::thread& t : th) t.join();
+  int first = FMT2D_OK;
+  for (int i = 0; i < n; ++i) {
+    if (status) status[i] = rc[i];
+    if (first == FMT2D_OK && rc[i] != FMT2D_OK) first = rc[i];
+  }
+  return first;
 }
 
 int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* gx, double* gz) {

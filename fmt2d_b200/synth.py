@@ -138,3 +138,56 @@ def small_model(nx: int = 121, dx: float = 0.25, zrel_max: float = 8.0, nzs: int
                               moho_wavelength=15.0, cb_dx=5.0, cb_dz=2.5, cb_amp=cb_amp,
                               seed=seed, phases=phases, max_offset=max_offset, name="small",
                               lc_thick=3.0)
+
+
+def _grf(rng, nz: int, nx: int, dz: float, dx: float, corr: float) -> np.ndarray:
+    """Gaussian random field on an nz x nx grid with a Gaussian correlation of
+    length corr (km), unit standard deviation (spectral filtering of white
+    noise)."""
+    w = rng.standard_normal((nz, nx))
+    kz = np.fft.fftfreq(nz, d=dz)[:, None]
+    kx = np.fft.fftfreq(nx, d=dx)[None, :]
+    filt = np.exp(-(np.pi * corr) ** 2 * (kx * kx + kz * kz))
+    f = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+    s = f.std()
+    return f / s if s > 0 else f
+
+
+def uneven_model(k: int, max_obs: int = 40) -> SmeshModel:
+    """Model k of the uneven-size multi-model batch (seed 100 + k): grid sizes
+    drawn uniformly from 401x121 to 2001x401 at 0.1 to 0.25 km spacing; a
+    random 1-D velocity gradient with a 3 to 8% Gaussian-random-field
+    perturbation (correlation length 5 km); a sediment layer 1 to 3 km thick
+    below the seafloor at 1.8 to 3.0 km/s; a Moho at 14 to 22 km; 10 to
+    max_obs OBS.  Every phase can be traced (water, sediment and Moho are all
+    present)."""
+    rng = np.random.default_rng(100 + k)
+    dx = float(rng.uniform(0.1, 0.25))
+    nx = int(rng.integers(401, 2002))
+    nz_target = int(rng.integers(121, 402))
+    topo_mean = float(rng.uniform(2.0, 3.5))
+    xpos = dx * np.arange(nx, dtype=np.float64)
+    topo = topo_mean + 0.5 * np.sin(2 * np.pi * xpos / float(rng.uniform(30.0, 80.0)))
+    zmax = (nz_target - 1) * dx
+    zrel_max = max(8.0, zmax - topo.max() - 5.0)
+    nzs = max(16, int(zrel_max / 0.25) + 1)
+    zrel = np.linspace(0.0, zrel_max, nzs)
+    X, ZR = np.meshgrid(xpos, zrel)
+    sed_th = float(rng.uniform(1.0, 3.0))
+    v_sed = float(rng.uniform(1.8, 3.0))
+    v0, grad = float(rng.uniform(4.2, 5.2)), float(rng.uniform(0.08, 0.14))
+    vel = np.minimum(v0 + grad * ZR, 7.6)
+    amp = float(rng.uniform(0.03, 0.08))
+    vel = vel * (1.0 + amp * np.clip(_grf(rng, nzs, nx, zrel[1] - zrel[0], dx, 5.0), -3, 3) / 3)
+    vel = np.where(ZR < sed_th, v_sed + (ZR / sed_th) * 0.3, vel)
+    moho_base = min(float(rng.uniform(14.0, 22.0)), topo.max() + zrel_max - 2.0)
+    moho = moho_base + float(rng.uniform(0.3, 1.5)) * np.sin(2 * np.pi * xpos / 40.0)
+    zabs = ZR + topo[None, :]
+    vel = np.where(zabs >= moho[None, :], 8.0, vel)
+    sed = topo + sed_th
+    n_obs = int(rng.integers(10, max_obs + 1))
+    width = xpos[-1]
+    obs_x = np.round(np.linspace(0.05 * width, 0.95 * width, n_obs) / dx) * dx
+    obs_x = np.clip(obs_x, xpos[1], xpos[-2])
+    return SmeshModel(xpos=xpos, topo=topo, zrel=zrel, vel=vel, vwater=1.5, sed_z=sed,
+                      moho_z=moho, obs_x=obs_x, name=f"uneven-{k}")

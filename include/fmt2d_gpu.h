@@ -191,6 +191,16 @@ FMT2D_API int fmt2d_gauss_smooth(fmt2d_ctx* ctx, int which, double corr_x, doubl
 /* Solve every time field of the enabled phases (bit p-1 of phase_mask enables
  * phase p) for nsrc OBS sources placed on the seafloor below src_x[s]. */
 FMT2D_API int fmt2d_forward(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask);
+/* fmt2d_forward of n contexts at once (one model each, of any grid size):
+ * context i solves nsrc[i] sources at src_x[i] for phase_mask[i].  The
+ * contexts' stage chains run concurrently on their own streams, so the
+ * fields of many small or uneven models fill the device together instead of
+ * one model after another (the reference runs run_forward2d once per model,
+ * src/inversion2d.f90:4145-4545).  The contexts must be distinct and on one
+ * device or several; status[i] (may be NULL) receives each forward's code,
+ * the return value is the first failure (its context holds the message). */
+FMT2D_API int fmt2d_forward_batch(fmt2d_ctx* const* ctxs, int n, const double* const* src_x,
+                                  const int* nsrc, const int* phase_mask, int* status);
 /* Time field tf (1..12) of source s in its region's node order, FP64; any of
  * T, dtdx, dtdz may be NULL.  Unreached nodes hold 1e20. */
 FMT2D_API int fmt2d_get_field(fmt2d_ctx* ctx, int src, int tf, double* T, double* dtdx, double* dtdz);
