@@ -194,8 +194,9 @@ def measured_peak_hbm():
 
 
 # DRAM bytes (read + write) per region node of the field solve (k_solve), from
-# an ncu capture of one launch (None until one is summarised under profiles/)
-K_SOLVE_DRAM_BYTES_PER_NODE = None
+# an ncu capture of one launch on 4 Pg fields of this model (2,581,316 region
+# nodes, 163.5 MB read + 127.6 MB written): profiles/k_solve_2001x401_pg_4src.md
+K_SOLVE_DRAM_BYTES_PER_NODE = 112.8
 
 
 def traffic_per_step(nodes_step: float):
