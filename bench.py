@@ -361,40 +361,56 @@ def rays_and_lsqr(g, m, stream):
     return rays, lsqr
 
 
-def inversion_iterations(local, n_iter: int = 2):
-    """Seconds per outer inversion iteration on the 2001x401 model (the
-    lsqr_inversion2d loop body, fmt2d_b200.inversion): observed times are the
-    checkerboard model's (device forward + rays, seeded 40 ms noise), the
-    inversion starts from the smooth model with a flat Moho; fixed damping 1,
-    Laplacian smoothing 10, alternating velocity / interface schedule.  Each
-    iteration: forward + rays + Frechet rows, selection, LSQR, line-search
-    forwards with model steps."""
+def inversion_iterations(local, n_iter: int = 2, cfg: int = 1):
+    """Seconds per outer inversion iteration (the lsqr_inversion2d loop body,
+    fmt2d_b200.inversion) through the public API.  Observed times are the
+    checkerboard model's (device forward + rays, seeded Gaussian noise), the
+    inversion starts from the smooth model with a flat Moho, alternating
+    velocity / interface updates.  cfg 1: the 2001x401 model, 30 OBS, Pg+PmP,
+    40 ms noise, fixed damping 1, Laplacian smoothing 10.  cfg 4: the 4001x601
+    model, 100 OBS, all five phases, 30-60 ms noise by phase, auto damping
+    and hybrid smoothing.  Each iteration: forward + rays + Frechet rows,
+    selection, damped LSQR solves, line-search forwards with model steps."""
     from fmt2d_b200 import synth
     from fmt2d_b200.api import Fmt2d
     from fmt2d_b200.inversion import Inversion, InversionParams
-    true, start = synth.config(1), synth.start_model(1)
+    true, start = synth.config(cfg), synth.start_model(cfg)
     P = true.picks
+    if cfg == 4:
+        phases = (1, 2, 3, 4, 5)
+        sigma = np.array([0.0, 0.030, 0.040, 0.050, 0.060, 0.060])[P[:, 1].astype(int)]
+        params = InversionParams(phases=phases, lam_damp=0.0, lam_smooth=10.0,
+                                 lam_smooth_iface=10.0, smooth_type=3, corr_x_iface=2.0,
+                                 lsqr_max_iter=500, crit_chi=1.0, alt_inv_mode=-1)
+    else:
+        phases = PHASES
+        sigma = np.full(P.shape[0], 0.040)
+        params = InversionParams(phases=phases, lam_damp=1.0, lam_smooth=10.0,
+                                 lam_smooth_iface=10.0, crit_chi=1.0, alt_inv_mode=-1)
+    t0 = time.perf_counter()
     g = Fmt2d(local).upload(true)
-    g.forward(true.obs_x, PHASES)
+    g.forward(true.obs_x, phases)
     t, valid, _ = g.trace(P[:, 0].astype(np.int32), P[:, 1].astype(np.int32), P[:, 2], P[:, 3])
     g.close()
-    rng = np.random.default_rng(1)
-    obs = np.where(valid, t + rng.normal(0.0, 0.040, t.size), -1.0)
+    rng = np.random.default_rng(cfg)
+    obs = np.where(valid, t + rng.normal(0.0, 1.0, t.size) * sigma, -1.0)
+    t_obs = time.perf_counter() - t0
     g = Fmt2d(local).upload(start)
-    inv = Inversion(g, start.obs_x, P, obs,
-                    InversionParams(phases=PHASES, lam_damp=1.0, lam_smooth=10.0,
-                                    lam_smooth_iface=10.0, crit_chi=1.0, alt_inv_mode=-1))
+    inv = Inversion(g, start.obs_x, P, obs, params)
     rows = []
     for _ in range(n_iter):
         r = inv.iteration()
         rows.append({"s": round(r.seconds, 3), "rms_orig_ms": round(1e3 * r.rms_orig, 3),
                      "rms_new_ms": round(1e3 * r.rms_new, 3), "step": r.step, "ndata": r.ndata,
-                     "forwards": r.forwards, "lsqr_solves": r.lsqr_solves,
+                     "mode": r.mode, "forwards": r.forwards, "lsqr_solves": r.lsqr_solves,
                      "phases_s": {k: round(v, 3) for k, v in r.phases_s.items()}})
     g.close()
+    grid = f"{true.nx}x{synth.config(cfg).pgrid_nz()}"
     return {"value": round(float(np.mean([x["s"] for x in rows])), 3),
             "unit": "s per inversion iteration", "iterations": rows,
-            "workload": "2001x401, 30 OBS, Pg+PmP, 29344 picks, start: smooth model, flat Moho",
+            "workload": f"config {cfg}: {grid}, {true.obs_x.size} OBS, phases {phases}, "
+                        f"{P.shape[0]} picks, start: smooth model, flat Moho",
+            "observed_times_s": round(t_obs, 3),
             "note": "wall clock through the public API, 1 GPU"}
 
 
@@ -545,7 +561,7 @@ def run_ours(args, world, rank, local):
     inversion = None
     if world == 1 and not args.no_inversion:
         try:
-            inversion = inversion_iterations(local)
+            inversion = inversion_iterations(local, args.inversion_iters, args.inversion_config)
         except Exception as ex:
             inversion = {"unavailable": str(ex)[:200]}
 
@@ -615,6 +631,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-inversion", action="store_true",
                     help="skip the s-per-inversion-iteration leg")
+    ap.add_argument("--inversion-config", type=int, default=1, choices=[1, 4],
+                    help="model of the inversion leg: 1 (2001x401) or 4 (4001x601, minutes)")
+    ap.add_argument("--inversion-iters", type=int, default=2)
     ap.add_argument("--models", type=int, default=8,
                     help="models of the uneven multi-model batch leg (0: skip)")
     ap.add_argument("--sources", type=int, default=0,

@@ -104,7 +104,7 @@ __host__ __device__ inline int tiles_of(const Fld64& F) {
 // smem_bits is the bitset size in words that fits, larger fields use their
 // global bitsets.
 __global__ void __launch_bounds__(kSolveThreads, 1)
-    k_solve(Fld64* fields, int nf, int smem_bits, int tiles_cap, long long max_steps,
+    k_solve(Fld64* fields, int nf, int smem_bits, int nsmem, int tiles_cap, long long max_steps,
             unsigned long long* ctr) {
   extern __shared__ __align__(16) unsigned char dsm_raw[];
   __shared__ SolveShared sh;
@@ -133,10 +133,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   unsigned* scl = sl[1] + kLCap;
   unsigned short* ready = reinterpret_cast<unsigned short*>(scl + kCCap);
   unsigned* sbits = reinterpret_cast<unsigned*>(ready + tiles_cap);
-  const bool local_bits = nbw <= (unsigned)smem_bits;
-  unsigned* bits = local_bits ? sbits : F.inq;
-  unsigned* wbits = local_bits ? sbits + smem_bits : F.wait;
-  unsigned* mbits = local_bits ? sbits + 2 * smem_bits : F.moving;
+  // the bitsets in shared memory, as many as fit in order of use: listed
+  // (atomics on every push), moving (read by arbitration), waiting
+  const int nloc = nbw <= (unsigned)smem_bits ? nsmem : 0;
+  unsigned* bits = nloc >= 1 ? sbits : F.inq;
+  unsigned* mbits = nloc >= 2 ? sbits + smem_bits : F.moving;
+  unsigned* wbits = nloc >= 3 ? sbits + 2 * smem_bits : F.wait;
+  // a field without a window never holds a node back: nothing waits
+  const bool windowed = F.clock[1] < kReachD;
   unsigned* ov[2] = {F.over, F.over + ns};
   unsigned* cov = F.over + 2 * (size_t)ns;
   for (unsigned w = tid; w < nbw; w += kSolveThreads) {
@@ -172,9 +176,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
     for (unsigned i = tid; i < n; i += kSolveThreads) {
       const unsigned s = get_entry(sl[cur], ov[cur], i);
       atomicAnd(bits + (s >> 5), ~(1u << (s & 31)));
+      const uint32_t code = FMT_RO(F.code + s);
       const NewV nv = evaluate(F, (int)s);
       ++n_eval;
-      if (!(FMT_RO(F.code + s) & kFullyRegular)) {
+      if (!(code & kFullyRegular)) {
         ++n_cut;
         sh.cutstep[par] = 1;
       }
@@ -278,7 +283,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       if (t < 0) continue;
       const double thr = fmin(F.Tn[s], F.T[s]);
       // a waiting target (its bit may be stale) drops the time it waits with
-      const bool waiting = (wbits[t >> 5] >> (t & 31)) & 1u;
+      const bool waiting = windowed && ((wbits[t >> 5] >> (t & 31)) & 1u);
       if (waiting) F.pend[t] = -1.0;
       if (waiting || !(F.T[t] < thr)) push(bits, sl[nxt], ov[nxt], &sh.cnt[nxt], (unsigned)t);
     }
@@ -680,18 +685,22 @@ void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, cudaStrea
 }
 // Dynamic shared memory of k_solve for a batch whose largest field has
 // max_slots slots and max_tiles tiles (tiles_cap rounded up to a multiple of
-// 8); smem_bits: words of each bitset kept in shared memory (0: global).
-static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* tiles_cap) {
+// 8); smem_bits: words of each bitset kept in shared memory, nsmem: how many
+// of the three bitsets (listed, moving, waiting, in that order) fit there
+// (0: all in global memory).
+static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* nsmem,
+                         int* tiles_cap) {
   const int cap = (max_tiles + 7) / 8 * 8;
   const size_t fixed = (size_t)cap * sizeof(unsigned long long) +
                        (2 * (size_t)kLCap + kCCap) * sizeof(unsigned) +
                        (size_t)cap * sizeof(unsigned short);
   const size_t nbw = (max_slots + 31) / 32;
-  const size_t room = fixed + 1024 < kSmemMax ? (kSmemMax - fixed - 1024) / (3 * sizeof(unsigned)) : 0;
-  const size_t words = nbw <= room ? nbw : 0;   // the three bitsets of every field fit, or none
-  *smem_bits = (int)words;
+  const size_t room = fixed + 1024 < kSmemMax ? (kSmemMax - fixed - 1024) / sizeof(unsigned) : 0;
+  const int n = nbw == 0 ? 0 : (int)std::min<size_t>(3, room / nbw);
+  *smem_bits = n > 0 ? (int)nbw : 0;
+  *nsmem = n;
   *tiles_cap = cap;
-  return fixed + 3 * words * sizeof(unsigned);
+  return fixed + (size_t)n * nbw * sizeof(unsigned);
 }
 int e64_tiles(const Fld64& f) { return tiles_of(f); }
 int e64_tiles_max() { return kTilesMax; }
@@ -720,10 +729,10 @@ static void solve_attr_once() {
 }
 void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
                unsigned long long* ctr, cudaStream_t st) {
-  int smem_bits = 0, cap = 0;
-  const size_t bytes = solve_smem(max_slots, max_tiles, &smem_bits, &cap);
+  int smem_bits = 0, nsmem = 0, cap = 0;
+  const size_t bytes = solve_smem(max_slots, max_tiles, &smem_bits, &nsmem, &cap);
   solve_attr_once();
-  k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, cap, max_steps, ctr);
+  k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, nsmem, cap, max_steps, ctr);
 }
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st) {
   const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 512);

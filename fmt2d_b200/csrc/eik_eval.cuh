@@ -440,23 +440,27 @@ FMT_HD void from_2(const Mem& n1, const Mem& n2, double xu, double zu, double vu
 // members accepted by then (p included) in that order; update_time2d swaps p
 // to the front and calls time_from_1 (p), then time_from_2 (p, list[k]) for
 // k = 1.. of the swapped list.
+// The events triggered by member p of a cut cell (its acceptance).
+FMT_HD void cut_member(const Mem* m, int nm, int p, double xu, double zu, double vu, double tol,
+                       int cbase, CutAcc& A) {
+  if (!m[p].single_ok) return;
+  int lst[6], n = 0, pp = 0;
+  for (int q = 0; q < nm; ++q) {
+    const bool before = q == p || m[q].T < m[p].T || (m[q].T == m[p].T && q < p);
+    if (!before) continue;
+    if (q == p) pp = n;
+    lst[n++] = q;
+  }
+  from_1(m[p], xu, zu, vu, tol, m[p].T, cbase, A);
+  for (int k = 1; k < n; ++k) {
+    const int q = (k == pp) ? lst[0] : lst[k];
+    from_2(m[p], m[q], xu, zu, vu, tol, cbase + k, A);
+  }
+}
+
 FMT_HD void cut_cell(const Mem* m, int nm, double xu, double zu, double vu, double tol,
                          int cbase, CutAcc& A) {
-  for (int p = 0; p < nm; ++p) {
-    if (!m[p].single_ok) continue;
-    int lst[6], n = 0, pp = 0;
-    for (int q = 0; q < nm; ++q) {
-      const bool before = q == p || m[q].T < m[p].T || (m[q].T == m[p].T && q < p);
-      if (!before) continue;
-      if (q == p) pp = n;
-      lst[n++] = q;
-    }
-    from_1(m[p], xu, zu, vu, tol, m[p].T, cbase, A);
-    for (int k = 1; k < n; ++k) {
-      const int q = (k == pp) ? lst[0] : lst[k];
-      from_2(m[p], m[q], xu, zu, vu, tol, cbase + k, A);
-    }
-  }
+  for (int p = 0; p < nm; ++p) cut_member(m, nm, p, xu, zu, vu, tol, cbase, A);
 }
 
 FMT_HD inline bool member_at(const Fld64& F, int brow, int col, Mem& m) {
@@ -556,6 +560,23 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
   return o;
 }
 
+// Members of connected cut cell q of grid node (r, c), in the reference's
+// connected-node order: the top and bottom interface nodes the cell carries,
+// then its corners other than the node itself.
+FMT_HD inline int cell_members(const Fld64& F, int r, int c, uint32_t code, int q, Mem* m) {
+  const int ci = r - ((q & 1) ? 1 : 0), cj = c - (q >= 2 ? 1 : 0);
+  int nm = 0;
+  if ((code & (1u << (12 + q))) && member_iface(F, 0, cj, m[nm])) ++nm;
+  if ((code & (1u << (16 + q))) && member_iface(F, 1, cj, m[nm])) ++nm;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      const int rr = ci + b, cc = cj + a;
+      if (rr == r && cc == c) continue;
+      if (member_at(F, rr, cc, m[nm])) ++nm;
+    }
+  return nm;
+}
+
 // Update of the grid node at bbox row r, column c.
 FMT_HD NewV update_grid(const Fld64& F, int r, int c) {
   NewV none;
@@ -593,17 +614,8 @@ FMT_HD NewV update_grid(const Fld64& F, int r, int c) {
 #pragma unroll 1
   for (int q = 0; q < 4; ++q) {
     if (!(code & (1u << (4 + q))) || !(code & (1u << (8 + q)))) continue;
-    const int ci = r - ((q & 1) ? 1 : 0), cj = c - (q >= 2 ? 1 : 0);
     Mem m[6];
-    int nm = 0;
-    if ((code & (1u << (12 + q))) && member_iface(F, 0, cj, m[nm])) ++nm;
-    if ((code & (1u << (16 + q))) && member_iface(F, 1, cj, m[nm])) ++nm;
-    for (int a = 0; a < 2; ++a)
-      for (int b = 0; b < 2; ++b) {
-        const int rr = ci + b, cc = cj + a;
-        if (rr == r && cc == c) continue;
-        if (member_at(F, rr, cc, m[nm])) ++nm;
-      }
+    const int nm = cell_members(F, r, c, code, q, m);
     cut_cell(m, nm, xu, zu, vu, F.tol, q * 32, A);
   }
   const bool reg_wins = rb.t < A.best.t || (rb.t == A.best.t && earlier(rb.trig, rb.ord, A.best));

@@ -139,3 +139,106 @@ def model_from_files(smesh: str, sed: str, moho: str, geom: str | None = None,
                    vwater=sm["vwater"], sed_z=iface_on_grid(xs, zs, sm["xpos"]),
                    moho_z=iface_on_grid(xm, zm, sm["xpos"]), obs_x=obs_x, picks=picks, name=name)
     return m, g
+
+
+# ---------------------------------------------------------------- output files
+def _rows(values, per_line: int, fmt: str) -> str:
+    """Fortran '(nFw.d)' output: per_line values a record."""
+    v = list(values)
+    return "".join("".join(format(x, fmt) for x in v[i:i + per_line]) + "\n"
+                   for i in range(0, len(v), per_line)) if v else "\n"
+
+
+def smesh_from_grid(xpos, seafloor, zrel, zgrid, vel_grid, active):
+    """The velocity of the inversion grid sampled back onto the smesh layout
+    (depth zrel below the seafloor), write_model2d's rule
+    (src/inversion2d.f90:3866-3901): at z = seafloor + zrel, linear between
+    the bracketing grid rows, taking the lower row alone when the upper one is
+    inactive or slower than 2 km/s (no interpolation across the seafloor);
+    clamped to the first / last row outside the grid.  vel_grid, active:
+    (nz, nx).  Returns (nzs, nx)."""
+    xpos = np.asarray(xpos, dtype=np.float64)
+    zrel = np.asarray(zrel, dtype=np.float64)
+    zg = np.asarray(zgrid, dtype=np.float64)
+    V = np.asarray(vel_grid, dtype=np.float64)
+    A = np.asarray(active, dtype=bool)
+    nz = zg.size
+    out = np.zeros((zrel.size, xpos.size))
+    for ix in range(xpos.size):
+        for iz, zr in enumerate(zrel):
+            z = seafloor[ix] + zr
+            lo, hi = 0, nz - 1
+            for k in range(nz - 1):
+                if zg[k] <= z <= zg[k + 1]:
+                    lo, hi = k, k + 1
+                    break
+            if z <= zg[0]:
+                v = V[0, ix]
+            elif z >= zg[nz - 1]:
+                v = V[nz - 1, ix]
+            else:
+                w = (z - zg[lo]) / (zg[hi] - zg[lo])
+                if A[lo, ix] and V[lo, ix] >= 2.0:
+                    v = (1.0 - w) * V[lo, ix] + w * V[hi, ix]
+                else:
+                    v = V[hi, ix]
+            out[iz, ix] = v
+    return out
+
+
+def write_model(directory: str, g, iteration: int, zrel, vwater: float, vair: float = 0.33):
+    """write_model2d (src/inversion2d.f90:3842-3962) for a context's current
+    model: vgrid_1_vtype1.smesh (the velocity back on the input smesh's
+    relative depths), iface_<k>.refl of the inverted interface, and
+    model_iter<iteration>.dat (the grid velocity by column and the interface
+    depths).  These files restart an inversion (`model_from_files`)."""
+    import os
+    inv, nvp, npar = g.inv_index()
+    vel = g.velocity()                         # (nz, nx)
+    nz, nx = vel.shape
+    xpos = np.asarray(g.model.xpos, dtype=np.float64)
+    seafloor = g.interface(2)
+    zgrid = np.arange(nz) * g.dx
+    zrel = np.asarray(zrel, dtype=np.float64)
+    sm = smesh_from_grid(xpos, seafloor, zrel, zgrid, vel, inv > 0)
+    with open(os.path.join(directory, "vgrid_1_vtype1.smesh"), "w") as f:
+        f.write(f"{nx:6d}{zrel.size:6d}{vwater:10.3f}{vair:10.3f}\n")
+        f.write(_rows(xpos, 10, "12.4f"))
+        f.write(_rows(seafloor, 10, "12.4f"))
+        f.write(_rows(zrel, 10, "12.4f"))
+        for ix in range(nx):
+            f.write("".join(format(v, "10.4f") for v in sm[:, ix]) + "\n")
+    k = int(getattr(g, "iface_inv", 4))
+    zi = g.interface(k) if npar > nvp else None
+    if zi is not None:
+        with open(os.path.join(directory, f"iface_{k}.refl"), "w") as f:
+            for x, z in zip(xpos, zi):
+                f.write(f"{x:12.3f}{z:12.3f}\n")
+    with open(os.path.join(directory, f"model_iter{int(iteration)}.dat"), "w") as f:
+        f.write(f"Iteration {int(iteration)}\n")
+        f.write("vgrid 1 vtype 1\n")
+        for ix in range(nx):
+            f.write(_rows(vel[:, ix], 10, "10.4f"))
+        if zi is not None:
+            f.write(f"iface {k}\n")
+            f.write(_rows(zi, 10, "12.4f"))
+
+
+def write_residuals(path: str, src, rcv_x, rcv_z, phase, obs, t_calc, valid):
+    """write_residuals2d (src/inversion2d.f90:3342-3377): one line per valid
+    pick with an observation (src_id is 1-based, as the reference numbers its
+    sources)."""
+    keep = np.asarray(valid, dtype=bool) & (np.asarray(obs) >= 0.0)
+    with open(path, "w") as f:
+        f.write("# src_id  rcv_x  rcv_z  phase_id  obs_time  calc_time  residual\n")
+        for i in np.flatnonzero(keep):
+            o, c = float(obs[i]), float(t_calc[i])
+            f.write(f"{int(src[i]) + 1:6d}{float(rcv_x[i]):12.3f}{float(rcv_z[i]):10.3f}"
+                    f"{int(phase[i]):4d}{o:12.6f}{c:12.6f}{_es14_6(o - c)}\n")
+    return int(keep.sum())
+
+
+def _es14_6(x: float) -> str:
+    """Fortran ES14.6: d.dddddde+xx right-justified in 14 columns."""
+    m, e = f"{x:.6e}".split("e")
+    return f"{m}E{int(e):+03d}".rjust(14)
