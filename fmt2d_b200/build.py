@@ -6,6 +6,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_lib")
@@ -20,23 +21,28 @@ def build(jobs: int = 8) -> str:
 
 def build_torch_ops() -> str:
     """Compile csrc/torch_ops.cpp against torch and libfmt2d_b200.so (in-tree,
-    rpath to _lib) into _lib/libfmt2d_torch.so.  The link line runs under ninja
-    and a shell: $$ is ninja's literal dollar sign, the quotes keep the shell
-    from expanding $ORIGIN."""
+    rpath to _lib) into _lib/libfmt2d_torch.so.  The compile runs in a child
+    process: torch.utils.cpp_extension loads what it builds, and a second
+    library registering the fmt2d operators in the caller's process would
+    abort it."""
     src = os.path.join(HERE, "csrc", "torch_ops.cpp")
     if os.path.exists(TORCH_OPS) and os.path.getmtime(TORCH_OPS) >= max(
             os.path.getmtime(src), os.path.getmtime(os.path.join(LIB, "libfmt2d_b200.so"))):
         return TORCH_OPS
-    from torch.utils import cpp_extension as ce
     bdir = os.path.join(HERE, "_build", "torch_ops")
     os.makedirs(bdir, exist_ok=True)
-    out = ce.load(name="fmt2d_torch", sources=[src], build_directory=bdir,
-                  is_python_module=False, with_cuda=True, verbose=False,
-                  extra_cflags=["-O2", "-std=c++17"],
-                  extra_ldflags=[f"-L{LIB}", "-lfmt2d_b200", "'-Wl,-rpath,$$ORIGIN'",
-                                 "'-Wl,-rpath,$$ORIGIN/../../_lib'"])
-    built = out if isinstance(out, str) else os.path.join(bdir, "fmt2d_torch.so")
-    shutil.copy2(built, TORCH_OPS)
+    # The link line runs under ninja and a shell: $$ is ninja's literal dollar
+    # sign, the quotes keep the shell from expanding $ORIGIN.
+    code = (
+        "import sys\n"
+        "from torch.utils import cpp_extension as ce\n"
+        "out = ce.load(name='fmt2d_torch', sources=[sys.argv[1]], build_directory=sys.argv[2],\n"
+        "              is_python_module=False, with_cuda=True, verbose=False,\n"
+        "              extra_cflags=['-O2', '-std=c++17'],\n"
+        "              extra_ldflags=['-L' + sys.argv[3], '-lfmt2d_b200',\n"
+        "                             \"'-Wl,-rpath,$$ORIGIN'\", \"'-Wl,-rpath,$$ORIGIN/../../_lib'\"])\n")
+    subprocess.run([sys.executable, "-c", code, src, bdir, LIB], check=True)
+    shutil.copy2(os.path.join(bdir, "fmt2d_torch.so"), TORCH_OPS)
     return TORCH_OPS
 
 

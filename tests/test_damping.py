@@ -120,5 +120,5 @@ def test_api_wrapper_plumbing(oracle_lib):
                       w_smooth_iface=1.5, eps_min=1e-9, max_iter=50)
     assert len(seen) == 1
     assert seen[0] == dict(wdv=3.0, wdv_iface=0.5, w_smooth=2.0, w_smooth_iface=1.5,
-                           eps_min=1e-9, max_iter=50)
+                           eps_min=1e-9, max_iter=50, smooth_type=1)
     assert r.dm.shape == (npar,) and r.wdv == 3.0 and r.wdv_iface == 0.5
