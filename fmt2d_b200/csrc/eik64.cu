@@ -205,7 +205,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
       if (nv.spread) {
         sh.changed[par] = 1;
         F.claim[s] = dbits(nv.T);
-        F.uses[s] = nv.uses;
         atomicOr(mbits + (s >> 5), 1u << (s & 31));
       }
     }
@@ -246,9 +245,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
         if (t >= 0 && ((mbits[t >> 5] >> (t & 31)) & 1u)) {
           const unsigned long long ks = F.claim[s], kt = F.claim[t];
           l = kt < ks || (kt == ks && t < s);
-#ifdef FMT2D_ARB_INPUTS
-          l = l && ((F.uses[s] >> hl) & 1u);
-#endif
         }
         lose = (__ballot_sync(hmask, l) & hmask) != 0u;
       }

@@ -40,7 +40,6 @@ struct Fld64 {
   uint8_t* fln = nullptr;           // new flags staged
   double* pend = nullptr;           // time a deferred node waits with (< 0: none)
   unsigned long long* claim = nullptr;   // bits of the new time of a node moving this step
-  uint16_t* uses = nullptr;         // neighbourhood positions of the staged value's inputs
   unsigned* list_in = nullptr;      // nodes to start from (seeds, re-listed nodes)
   unsigned* over = nullptr;         // 3*nslots: list overflow (two lists) and commit overflow
   unsigned* inq = nullptr;          // bitset over slots: listed (when not in shared memory)

@@ -83,7 +83,6 @@ struct Cand {
   double t, trig;
   double g0, g1, g2, g3, g4, g5;   // gradient operands, by kind (grad_of)
   int ord;
-  uint16_t uses;                   // neighbourhood positions (neighbour_slot) of its inputs
   uint8_t kind;
   bool gxi, gzi;                   // regular: the x / z neighbour took part
   bool sus, copy;
@@ -93,7 +92,7 @@ FMT_HD inline Cand no_cand() {
   Cand c;
   c.t = kHugeD; c.trig = kHugeD; c.ord = 0x7fffffff;
   c.g0 = c.g1 = c.g2 = c.g3 = c.g4 = c.g5 = 0.0;
-  c.kind = kGradNone; c.gxi = c.gzi = false; c.uses = 0;
+  c.kind = kGradNone; c.gxi = c.gzi = false;
   c.sus = false; c.copy = false;
   return c;
 }
@@ -143,7 +142,6 @@ FMT_HD inline void grad_of(const Cand& w, double& gx, double& gz) {
 // A direct neighbour of a grid node, as regular_update2d sees it.
 struct RNb {
   bool ok, single_ok, second, dirx;
-  uint8_t pos, pos2;               // neighbourhood positions of the node and its second neighbour
   double T, T2, d2, dpos;
 };
 
@@ -192,8 +190,6 @@ FMT_HD void rnb4(const Fld64& F, int r, int c, double vu, RNb* n) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     RNb& m = n[k];
-    m.pos = (uint8_t)(k == 0 ? 7 : k == 1 ? 8 : k == 2 ? 5 : 10);
-    m.pos2 = (uint8_t)(k == 0 ? 2 : k == 1 ? 3 : k == 2 ? 0 : 1);
     m.ok = false;
     m.second = false;
     m.dirx = dc[k] != 0;
@@ -279,12 +275,6 @@ FMT_HD bool reg_cand(const RNb* p, const RNb* q, Cand& o) {
   o.g3 = tz; o.g4 = t2z; o.g5 = dpz;
   o.sus = !(xi && zi);
   o.copy = false;
-  o.uses = 0;
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const RNb* n = k == 0 ? p : q;
-    if (n) o.uses |= (uint16_t)((1u << n->pos) | (n->second ? (1u << n->pos2) : 0u));
-  }
   return true;
 }
 
@@ -322,7 +312,6 @@ FMT_HD void quadrant(const RNb& X, const RNb& Z, int ord, Cand& best) {
 struct Mem {
   double x, z, T, gx, gz, v;
   bool single_ok, copied;
-  uint8_t pos;                     // neighbourhood position (neighbour_slot)
 };
 
 // Cut-cell candidates.  pre_min tracks the smallest cut-cell candidate that
@@ -362,7 +351,6 @@ FMT_HD void from_1(const Mem& a, double xu, double zu, double vu, double tol, do
   const double dxu = xu - a.x, dzu = zu - a.z;
   const double dist = sqrt(dxu * dxu + dzu * dzu);
   Cand c;
-  c.uses = (uint16_t)(1u << a.pos);
   if (dist < 0.01 * tol) {
     if (!a.copied) {
       given(c, a.gx, a.gz);
@@ -388,7 +376,6 @@ FMT_HD void from_2(const Mem& n1, const Mem& n2, double xu, double zu, double vu
   const double r1x = n1.x - xu, r1z = n1.z - zu;
   const double r2x = n2.x - xu, r2z = n2.z - zu;
   Cand c;
-  c.uses = (uint16_t)((1u << n1.pos) | (1u << n2.pos));
   if (sqrt(r1x * r1x + r1z * r1z) < 0.01 * tol) {
     if (!n1.copied) {
       given(c, n1.gx, n1.gz);
@@ -516,7 +503,6 @@ struct NewV {
   bool write, spread;   // store it; re-activate the stencil neighbours
   double T, gx, gz;
   bool sus, copy;
-  uint16_t uses;        // neighbourhood positions of the winner's inputs (0: the seed)
 };
 
 // Seeds precede every candidate in the reference's order; a seed at or below
@@ -540,13 +526,12 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
   grad_of(w, gx, gz);
   double T = w.t < kReachD ? w.t : kHugeD;
   bool su = sus, cp = w.copy;
-  uint16_t uses = w.uses;
   const uint8_t fl = ldF(F, s);
   if (fl & kFlSeed) {
     const double4 sd = F.seed[s];
     if (sd.x < kReachD) {
       if (T >= kReachD || sd.x <= T) {
-        T = sd.x; gx = sd.y; gz = sd.z; su = false; cp = false; uses = 0;
+        T = sd.x; gx = sd.y; gz = sd.z; su = false; cp = false;
       } else if (su && sd.x <= sus_t) {
         su = false;
       }
@@ -563,7 +548,7 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
   auto same = [](double a, double b) { return bits_of(a) == bits_of(b); };
   const bool gchg = !same(T, curT) || !same(gx, cg.x) || !same(gz, cg.y) ||
                     cp != ((fl & kFlCopy) != 0);
-  o.T = T; o.gx = gx; o.gz = gz; o.sus = su; o.copy = cp; o.uses = uses;
+  o.T = T; o.gx = gx; o.gz = gz; o.sus = su; o.copy = cp;
   o.spread = gchg;
   o.write = gchg || su != ((fl & kFlSusp) != 0);
   // with a change threshold, a move smaller than it (time in s, gradient in
@@ -581,18 +566,13 @@ FMT_HD NewV finish(const Fld64& F, int s, const Cand& w, bool sus, double sus_t)
 FMT_HD inline int cell_members(const Fld64& F, int r, int c, uint32_t code, int q, Mem* m) {
   const int ci = r - ((q & 1) ? 1 : 0), cj = c - (q >= 2 ? 1 : 0);
   int nm = 0;
-  // neighbourhood positions: interface nodes 12 + 2 side + (cj - c + 1), the
-  // 3x3 block 4..6 (row above), 7 / 8 (same row), 9..11 (row below)
-  if ((code & (1u << (12 + q))) && member_iface(F, 0, cj, m[nm])) m[nm++].pos = (uint8_t)(13 + cj - c);
-  if ((code & (1u << (16 + q))) && member_iface(F, 1, cj, m[nm])) m[nm++].pos = (uint8_t)(15 + cj - c);
+  if ((code & (1u << (12 + q))) && member_iface(F, 0, cj, m[nm])) ++nm;
+  if ((code & (1u << (16 + q))) && member_iface(F, 1, cj, m[nm])) ++nm;
   for (int a = 0; a < 2; ++a)
     for (int b = 0; b < 2; ++b) {
       const int rr = ci + b, cc = cj + a;
       if (rr == r && cc == c) continue;
-      if (member_at(F, rr, cc, m[nm])) {
-        const int dr = rr - r, dc = cc - c;
-        m[nm++].pos = (uint8_t)(dr < 0 ? 5 + dc : dr > 0 ? 10 + dc : (dc < 0 ? 7 : 8));
-      }
+      if (member_at(F, rr, cc, m[nm])) ++nm;
     }
   return nm;
 }
@@ -660,13 +640,11 @@ FMT_HD NewV update_iface(const Fld64& F, int side, int col) {
   int nm = 0;
   const int o = side ^ 1;
   const bool has_o = o == 0 ? (code & (1u << 12)) : (code & (1u << 16));
-  // neighbourhood positions: the other interface node 4, the cell's
-  // corners 2 a + b
-  if (has_o && member_iface(F, o, col, m[nm])) m[nm++].pos = 4;
+  if (has_o && member_iface(F, o, col, m[nm])) ++nm;
   const int br = izc - F.z_lo;
   for (int a = 0; a < 2; ++a)
     for (int b = 0; b < 2; ++b)
-      if (member_at(F, br + b, col + a, m[nm])) m[nm++].pos = (uint8_t)(2 * a + b);
+      if (member_at(F, br + b, col + a, m[nm])) ++nm;
   CutAcc A;
   A.best = no_cand();
   A.pre_min = kHugeD;

@@ -385,13 +385,12 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   L.sfln.alloc(total);
   L.spend.alloc(total * sizeof(double));
   L.sclaim.alloc(total * sizeof(unsigned long long));
-  L.suses.alloc(total * sizeof(uint16_t));
   L.slist.alloc(total * sizeof(unsigned));
   L.sover.alloc(3 * total * sizeof(unsigned));
   L.sinq.alloc(3 * words * sizeof(unsigned));
   L.scnt.alloc((size_t)nf * 4 * sizeof(unsigned));
   L.ctr.alloc(kCtrN * sizeof(unsigned long long));
-  if (!L.sTn.p || !L.sGn.p || !L.sfln.p || !L.spend.p || !L.sclaim.p || !L.suses.p || !L.slist.p ||
+  if (!L.sTn.p || !L.sGn.p || !L.sfln.p || !L.spend.p || !L.sclaim.p || !L.slist.p ||
       !L.sover.p ||
       !L.sinq.p || !L.scnt.p || !L.ctr.p)
     return "device allocation failed for the solver scratch";
@@ -406,7 +405,6 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     hf[i].fln = L.sfln.as<uint8_t>() + base;
     hf[i].pend = L.spend.as<double>() + base;
     hf[i].claim = L.sclaim.as<unsigned long long>() + base;
-    hf[i].uses = L.suses.as<uint16_t>() + base;
     hf[i].list_in = L.slist.as<unsigned>() + base;
     hf[i].over = L.sover.as<unsigned>() + 3 * base;
     hf[i].inq = L.sinq.as<unsigned>() + wbase;

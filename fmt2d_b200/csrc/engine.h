@@ -89,7 +89,7 @@ struct SolveLane {
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
   DevBuf fields, up, step, sx, sz, seeds, which, hw, ctr;
-  DevBuf sTn, sGn, sfln, spend, sclaim, suses, slist, sover, sinq, scnt;
+  DevBuf sTn, sGn, sfln, spend, sclaim, slist, sover, sinq, scnt;
   SolveStats stats;
   bool not_converged = false;
   // pinned staging of the lane's small host <-> device copies (descriptors,
@@ -100,7 +100,7 @@ struct SolveLane {
   size_t pin_cap = 0, pin_used = 0;
   void free_all() {
     for (DevBuf* b : {&fields, &up, &step, &sx, &sz, &seeds, &which, &hw, &ctr, &sTn, &sGn, &sfln,
-                      &spend, &sclaim, &suses, &slist, &sover, &sinq, &scnt})
+                      &spend, &sclaim, &slist, &sover, &sinq, &scnt})
       b->free_();
     if (pin) cudaFreeHost(pin);
     pin = nullptr;

@@ -74,6 +74,57 @@ __device__ int nearby_node(const TrModel& M, const TrRegion& r, int ix, int iz) 
   return -1;
 }
 
+// The region node nearest to (px, pz), the first in the reference's node
+// order among equals (grid nodes column by column, rows down each column,
+// then the top and the bottom interface nodes by column): what a scan of
+// every node with a strict "closer" test returns (rays2d.f90:966-972,
+// 1118-1127).  The region's grid nodes are one row range per column, so the
+// search widens column by column from the query and stops once a column's
+// horizontal distance alone exceeds the best distance found; each column
+// costs its nearest rows and its two interface nodes.
+__device__ int nearest_node(const TrModel& M, const TrRegion& r, double px, double pz) {
+  double best = 1.0e300;
+  int bcls = 3, bcol = 0, brow = 0, bslot = -1;
+  auto offer = [&](double d, int cls, int col, int row, int slot) {
+    if (d < best || (d == best && (cls < bcls || (cls == bcls && (col < bcol ||
+                                                  (col == bcol && row < brow)))))) {
+      best = d; bcls = cls; bcol = col; brow = row; bslot = slot;
+    }
+  };
+  const int nx = M.nx;
+  int c0 = (int)floor((px - M.x0) / M.dx);
+  c0 = max(0, min(nx - 1, c0));
+  const int fr = (int)floor(pz / M.dx);
+  // columns c0, c0 - 1, c0 + 1, c0 - 2, ...: the horizontal distance grows on
+  // each side, so once neither side's next column can hold a node as close as
+  // the best (d >= its horizontal term), no farther column can either
+  for (int k = 0;; ++k) {
+    bool near = false;
+    for (int side = 0; side < (k == 0 ? 1 : 2); ++side) {
+      const int c = side == 0 ? c0 - k : c0 + k;
+      if (c < 0 || c >= nx) continue;
+      const double gx = gxc(M, c + 1), xi = M.xpos[c];
+      if ((px - gx) * (px - gx) > best && (px - xi) * (px - xi) > best) continue;
+      near = true;
+      const int a = r.r0[c], b = r.r1[c];
+      if (a <= b) {
+#pragma unroll
+        for (int q = -1; q <= 2; ++q) {
+          const int row = min(b, max(a, fr + q));
+          const double z = gzc(M, row + 1);
+          offer((px - gx) * (px - gx) + (pz - z) * (pz - z), 0, c, row,
+                (row - r.z_lo) * r.pitch + c);
+        }
+      }
+      const double zt = M.ifz[r.itop][c], zb = M.ifz[r.ibot][c];
+      offer((px - xi) * (px - xi) + (pz - zt) * (pz - zt), 1, c, 0, r.H * r.pitch + c);
+      offer((px - xi) * (px - xi) + (pz - zb) * (pz - zb), 2, c, 0, (r.H + 1) * r.pitch + c);
+    }
+    if (!near && k > 0) break;
+  }
+  return bslot;
+}
+
 // rays2d.f90:1070-1131: nearest of the cell corners, else of every region
 // node (in the reference's node order).
 __device__ int position_in_region(const TrModel& M, const TrRegion& r, double px, double pz) {
@@ -93,16 +144,7 @@ __device__ int position_in_region(const TrModel& M, const TrRegion& r, double px
         if (d < dmin) { best = s; dmin = d; }
       }
     }
-  if (best < 0) {
-    dmin = 1.0e100;
-    for (int n = 0; n < r.nnode; ++n) {
-      const int s = r.slot_of_node[n];
-      double x, z;
-      node_pos(M, r, s, x, z);
-      const double d = (px - x) * (px - x) + (pz - z) * (pz - z);
-      if (d < dmin) { best = s; dmin = d; }
-    }
-  }
+  if (best < 0) best = nearest_node(M, r, px, pz);
   return best;
 }
 
@@ -159,15 +201,8 @@ __device__ double time_at(const TrModel& M, const TrRegion& r, const double* T, 
   if (t1 < hh && t2 < hh && t3 < hh && t4 < hh)
     return (1.0 - w1) * (1.0 - w2) * t1 + w1 * (1.0 - w2) * t2 + (1.0 - w1) * w2 * t3 +
            w1 * w2 * t4;
-  double t = kHugeT, dmin = kHugeT;
-  for (int n = 0; n < r.nnode; ++n) {
-    const int s = r.slot_of_node[n];
-    double x, z;
-    node_pos(M, r, s, x, z);
-    const double d = (px - x) * (px - x) + (pz - z) * (pz - z);
-    if (d < dmin) { dmin = d; t = T[s]; }
-  }
-  return t;
+  const int s = nearest_node(M, r, px, pz);
+  return s >= 0 ? T[s] : kHugeT;
 }
 
 // rays2d.f90:1222-1257

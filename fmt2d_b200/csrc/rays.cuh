@@ -9,6 +9,8 @@ namespace fmt2d {
 struct TrRegion {
   const uint32_t* code = nullptr;
   const int* slot_of_node = nullptr;   // region node id - 1 -> slot (the reference's node order)
+  const int* r0 = nullptr;             // per column: first / last grid row of the region
+  const int* r1 = nullptr;             // (absolute, 0-based; r1 < r0: none)
   int z_lo = 0, H = 0, pitch = 0, itop = 0, ibot = 0, id = 0, nnode = 0;
 };
 

@@ -72,6 +72,8 @@ std::string Engine::upload_trace_tables() {
     TrRegion& R = t.reg[r];
     R.code = reg_[r].code.as<uint32_t>();
     R.slot_of_node = reg_[r].slot_of_node.as<int>();
+    R.r0 = reg_[r].r0.as<int>();
+    R.r1 = reg_[r].r1.as<int>();
     R.z_lo = G.z_lo;
     R.H = G.H;
     R.pitch = G.pitch;

@@ -1,9 +1,10 @@
-"""The reference's input files (read_tomo2d.f90) for this library: readers
-(fmt2d_read_smesh / fmt2d_read_refl / fmt2d_read_geom, Fortran list-directed
-rules), writers of the same formats, and `model_from_files`, which turns a
-velocity mesh, the sediment-base and Moho files and a geometry file into the
-model descriptor and picks that `Fmt2d.upload` / `Fmt2d.forward` /
-`Fmt2d.trace` take."""
+"""The reference's files for this library: readers of its input files
+(read_tomo2d.f90; fmt2d_read_smesh / fmt2d_read_refl / fmt2d_read_geom,
+Fortran list-directed rules), writers of the same formats, `model_from_files`,
+which turns a velocity mesh, the sediment-base and Moho files and a geometry
+file into the model descriptor and picks that `Fmt2d.upload` /
+`Fmt2d.forward` / `Fmt2d.trace` take, and writers of the inversion's output
+files (write_model2d's smesh / refl / model_iter files, write_residuals2d)."""
 from __future__ import annotations
 
 import ctypes as C
