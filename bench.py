@@ -396,6 +396,7 @@ def inversion_iterations(local, n_iter: int = 2, cfg: int = 1):
     obs = np.where(valid, t + rng.normal(0.0, 1.0, t.size) * sigma, -1.0)
     t_obs = time.perf_counter() - t0
     g = Fmt2d(local).upload(start)
+    tune = g.autotune(start.obs_x, phases)
     inv = Inversion(g, start.obs_x, P, obs, params)
     rows = []
     for _ in range(n_iter):
@@ -410,7 +411,7 @@ def inversion_iterations(local, n_iter: int = 2, cfg: int = 1):
             "unit": "s per inversion iteration", "iterations": rows,
             "workload": f"config {cfg}: {grid}, {true.obs_x.size} OBS, phases {phases}, "
                         f"{P.shape[0]} picks, start: smooth model, flat Moho",
-            "observed_times_s": round(t_obs, 3),
+            "observed_times_s": round(t_obs, 3), "autotune": tune,
             "note": "wall clock through the public API, 1 GPU"}
 
 
@@ -481,6 +482,9 @@ def run_ours(args, world, rank, local):
     # the last stage of each phase (ray tracing starts there)
     terminal = sorted({{1: 1, 2: 3, 3: 5, 4: 8, 5: 12}[p] for p in PHASES})
 
+    # the solve block size for this workload (bit-identical results for every
+    # size), picked by the library's autotuner before the warm-up
+    tune = g.autotune(src, PHASES)
     for _ in range(args.warmup):
         g.forward(src, PHASES)
     torch.cuda.synchronize()
@@ -613,7 +617,7 @@ def run_ours(args, world, rank, local):
                         "algorithmic_bytes_per_step": alg_bytes,
                         "bytes_per_node": 16, "fp64_bytes_per_node": 36,
                         "fp64_frac": round(36.0 * nodes_step / (step_ms / 1e3) / 1e9 / peak, 7)},
-           "solver": solver,
+           "solver": solver, "autotune": tune,
            "rays": rays, "lsqr": lsqr, "inversion": inversion, "uneven_batch": batch,
            "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),

@@ -394,6 +394,24 @@ class Fmt2d:
                                               int(max_steps)), "fmt2d_set_schedule")
         return self
 
+    def set_solve_threads(self, threads: int = 0):
+        """Threads of each field's solve block (fmt2d_set_solve_threads): 256,
+        384 or 512, 0 for the default; results are identical for every size."""
+        self._check(self.L.fmt2d_set_solve_threads(self.h, int(threads)),
+                    "fmt2d_set_solve_threads")
+        return self
+
+    def autotune(self, src_x, phases=(1, 2, 3, 4, 5)) -> dict:
+        """Pick the fastest solve block size for this workload (fmt2d_autotune);
+        the context keeps it.  Returns {"threads": chosen, "ms": {size: ms}}."""
+        src_x = np.ascontiguousarray(src_x, dtype=np.float64)
+        t = C.c_int()
+        ms = np.zeros(3)
+        self._check(self.L.fmt2d_autotune(self.h, src_x, src_x.size, phase_mask(phases),
+                                          C.byref(t), N.ptr(ms)), "fmt2d_autotune")
+        self.mask, self.nsrc = phase_mask(phases), src_x.size
+        return {"threads": t.value, "ms": dict(zip((256, 384, 512), ms.round(3).tolist()))}
+
     def stream(self) -> int:
         """cudaStream_t (as an integer) that the context's work runs on."""
         s = C.c_void_p()

@@ -3,6 +3,7 @@
 #include "engine.h"
 #include "lsqr.h"
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -479,6 +480,49 @@ int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
   ctx->eng->window_cells = window_cells;
   ctx->eng->max_passes = max_passes;
   ctx->eng->max_steps = max_steps > 0 ? max_steps : fmt2d::Engine::kDefaultMaxSteps;
+  return FMT2D_OK;
+}
+
+int fmt2d_set_solve_threads(fmt2d_ctx* ctx, int threads) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  int n = 0;
+  const int* sizes = fmt2d::e64_solve_sizes(&n);
+  bool ok = threads == 0;
+  for (int k = 0; k < n; ++k) ok = ok || threads == sizes[k];
+  if (!ok) return ctx->fail(FMT2D_ERR_ARG, "solve block size must be 0 or one of 256, 384, 512");
+  ctx->eng->solve_threads = threads;
+  return FMT2D_OK;
+}
+
+int fmt2d_autotune(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask, int* threads,
+                   double* ms) {
+  if (!ctx || !src_x || nsrc <= 0 || (phase_mask & ~31) || !phase_mask) return FMT2D_ERR_ARG;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  int n = 0;
+  const int* sizes = fmt2d::e64_solve_sizes(&n);
+  // one untimed forward (field stores and solver scratch are allocated once)
+  std::string e = ctx->eng->forward(src_x, nsrc, phase_mask);
+  if (!e.empty())
+    return ctx->fail(ctx->eng->not_converged() ? FMT2D_ERR_CONVERGE : FMT2D_ERR_CUDA, e);
+  int best = 0;
+  double best_ms = 1.0e300;
+  for (int k = 0; k < n; ++k) {
+    ctx->eng->solve_threads = sizes[k];
+    const auto t0 = std::chrono::steady_clock::now();
+    e = ctx->eng->forward(src_x, nsrc, phase_mask);
+    const double t = std::chrono::duration<double, std::milli>(
+                         std::chrono::steady_clock::now() - t0).count();
+    if (!e.empty())
+      return ctx->fail(ctx->eng->not_converged() ? FMT2D_ERR_CONVERGE : FMT2D_ERR_CUDA, e);
+    if (ms) ms[k] = t;
+    if (t < best_ms) { best_ms = t; best = sizes[k]; }
+  }
+  ctx->eng->solve_threads = best;
+  if (threads) *threads = best;
   return FMT2D_OK;
 }
 

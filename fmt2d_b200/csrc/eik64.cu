@@ -40,12 +40,12 @@ namespace {
 using namespace ev;
 
 // ---------------------------------------------------------------- field solve
-#ifndef FMT2D_SOLVE_THREADS
-#define FMT2D_SOLVE_THREADS 384
-#endif
-constexpr int kSolveThreads = FMT2D_SOLVE_THREADS;   // threads of a field's solve block
-constexpr int kSolveWarps = kSolveThreads / 32;
-constexpr int kHalfWarps = kSolveThreads / 16;
+// Threads of a field's solve block: k_solve is instantiated for each size;
+// the result does not depend on it (no evaluation sees a value of its own
+// step), only the time does, so a context may pick the fastest for its
+// workload (e64_solve_sizes, fmt2d_autotune).
+constexpr int kSolveSizes[3] = {256, 384, 512};
+constexpr int kSolveDefault = 384;
 constexpr unsigned kLCap = 4096;          // entries of each list held in shared memory
 constexpr unsigned kCCap = 2048;          // commit entries held in shared memory
 constexpr int kTileRows = 8;              // a tile: 8 slot rows x 32 slot columns (one bitset word per row)
@@ -103,9 +103,12 @@ __host__ __device__ inline int tiles_of(const Fld64& F) {
 // list of tiles to scan, and (when they fit) the listed and waiting bitsets;
 // smem_bits is the bitset size in words that fits, larger fields use their
 // global bitsets.
+template <int kSolveThreads>
 __global__ void __launch_bounds__(kSolveThreads, 1)
     k_solve(Fld64* fields, int nf, int smem_bits, int nsmem, int tiles_cap, long long max_steps,
             unsigned long long* ctr) {
+  constexpr int kSolveWarps = kSolveThreads / 32;
+  constexpr int kHalfWarps = kSolveThreads / 16;
   extern __shared__ __align__(16) unsigned char dsm_raw[];
   __shared__ SolveShared sh;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -705,9 +708,10 @@ static size_t solve_smem(size_t max_slots, int max_tiles, int* smem_bits, int* n
 int e64_tiles(const Fld64& f) { return tiles_of(f); }
 int e64_tiles_max() { return kTilesMax; }
 // k_solve may use up to kSmemMax of dynamic shared memory.  The attribute is
-// set once per device: changing a kernel's attributes while it runs (a solve
-// of another stage chain on another stream) waits for that kernel to finish,
-// which would serialise the chains.
+// set once per device and instantiation: changing a kernel's attributes while
+// it runs (a solve of another stage chain on another stream) waits for that
+// kernel to finish, which would serialise the chains.
+template <int NT>
 static void solve_attr_once() {
   static std::mutex mu;
   static bool done[64] = {};
@@ -720,19 +724,36 @@ static void solve_attr_once() {
   int optin = 0;
   cudaFuncAttributes fa;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-      cudaFuncGetAttributes(&fa, k_solve) != cudaSuccess)
+      cudaFuncGetAttributes(&fa, k_solve<NT>) != cudaSuccess)
     return;
   const int dyn = std::min<int>((int)kSmemMax, optin - (int)fa.sharedSizeBytes);
-  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ==
+  if (cudaFuncSetAttribute(k_solve<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ==
       cudaSuccess)
     done[dev] = true;
 }
+
+template <int NT>
+static void solve_launch(Fld64* f, int nf, int smem_bits, int nsmem, int cap, size_t bytes,
+                         long long max_steps, unsigned long long* ctr, cudaStream_t st) {
+  solve_attr_once<NT>();
+  k_solve<NT><<<nf, NT, bytes, st>>>(f, nf, smem_bits, nsmem, cap, max_steps, ctr);
+}
+
+const int* e64_solve_sizes(int* n) {
+  *n = 3;
+  return kSolveSizes;
+}
+
 void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
-               unsigned long long* ctr, cudaStream_t st) {
+               unsigned long long* ctr, int threads, cudaStream_t st) {
   int smem_bits = 0, nsmem = 0, cap = 0;
   const size_t bytes = solve_smem(max_slots, max_tiles, &smem_bits, &nsmem, &cap);
-  solve_attr_once();
-  k_solve<<<nf, kSolveThreads, bytes, st>>>(f, nf, smem_bits, nsmem, cap, max_steps, ctr);
+  if (threads == 256)
+    solve_launch<256>(f, nf, smem_bits, nsmem, cap, bytes, max_steps, ctr, st);
+  else if (threads == 512)
+    solve_launch<512>(f, nf, smem_bits, nsmem, cap, bytes, max_steps, ctr, st);
+  else
+    solve_launch<kSolveDefault>(f, nf, smem_bits, nsmem, cap, bytes, max_steps, ctr, st);
 }
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st) {
   const int bx = (int)std::min<size_t>((max_slots + 255) / 256, 512);

@@ -96,8 +96,11 @@ void e64_start(Fld64* f, int nf, size_t max_slots, const double* step, cudaStrea
 // field, all steps in one launch; max_tiles: the most tiles of a field,
 // e64_tiles).  max_steps bounds the steps of a field;
 // a field that reaches it sets cnt[2] = 1.
+// threads: the solve block's size, one of e64_solve_sizes (others: the
+// default); the result does not depend on it.
 void e64_solve(Fld64* f, int nf, size_t max_slots, int max_tiles, long long max_steps,
-               unsigned long long* ctr, cudaStream_t st);
+               unsigned long long* ctr, int threads, cudaStream_t st);
+const int* e64_solve_sizes(int* n);
 // Tiles of a field's waiting-node index, and the most a field may have.
 int e64_tiles(const Fld64& f);
 int e64_tiles_max();

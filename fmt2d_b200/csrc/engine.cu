@@ -489,7 +489,7 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   cudaEventRecord(e0, L.st);
   unsigned long long bad = 0;
   for (int pass = 0;; ++pass) {
-    e64_solve(dF, nf, max_slots, max_tiles, max_steps, dctr, L.st);
+    e64_solve(dF, nf, max_slots, max_tiles, max_steps, dctr, solve_threads, L.st);
     ++L.stats.launches;
     ++L.stats.final_passes;
     cudaMemsetAsync(L.sinq.p, 0, words * sizeof(unsigned), L.st);

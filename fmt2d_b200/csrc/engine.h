@@ -140,6 +140,7 @@ class Engine {
   static constexpr long long kDefaultMaxSteps = 4000000;
   long long max_steps = kDefaultMaxSteps;  // safety cap on the steps of one field's solve
   int max_passes = 6;             // solve passes (each followed by a check of every node)
+  int solve_threads = 0;          // threads of a field's solve block (0: the default)
   // device pointers of a solved field (FP64 time, double2 final gradient per slot)
   const double* field_t(int src, int tf) const { return fields_[src][tf].T.as<double>(); }
   const double2* field_g(int src, int tf) const { return fields_[src][tf].Gout.as<double2>(); }

@@ -343,6 +343,19 @@ FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
 FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
                                  long long max_steps);
 
+/* Threads of each field's solve block: 256, 384 or 512 (0: the default,
+ * 384).  Results are the same bit for bit for every size (no evaluation of a
+ * solve step sees a value written in that step); only the time differs: larger
+ * blocks suit longer fronts (larger grids).  No reference counterpart. */
+FMT2D_API int fmt2d_set_solve_threads(fmt2d_ctx* ctx, int threads);
+/* Autotuner of the solve block size for a workload: one forward of nsrc
+ * sources for phase_mask, then one forward timed per block size; the fastest
+ * is kept for the context's later forwards and returned in *threads (may be
+ * NULL), the times in ms[0..2] (256, 384, 512; may be NULL).  The fields of
+ * the last forward stay valid.  No reference counterpart. */
+FMT2D_API int fmt2d_autotune(fmt2d_ctx* ctx, const double* src_x, int nsrc, int phase_mask,
+                             int* threads, double* ms);
+
 /* The CUDA stream (cudaStream_t) all work of the context is issued on, for
  * callers that record events around fmt2d_forward.  No reference counterpart. */
 FMT2D_API int fmt2d_stream(fmt2d_ctx* ctx, void** stream);

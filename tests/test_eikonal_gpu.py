@@ -159,3 +159,28 @@ def test_more_sources_after_fewer():
             a, b = g.field(s, tf), fresh.field(s, tf)
             for x, y in zip(a, b):
                 assert np.array_equal(x.view(np.int64), y.view(np.int64))
+
+
+def test_solve_block_sizes_identical_and_autotune():
+    """Every solve block size gives the same fields bit for bit (no
+    evaluation sees a value of its own step); the autotuner times each size,
+    keeps the fastest and leaves valid fields."""
+    from fmt2d_b200.api import Fmt2d, fields_of, phase_mask
+    m = synth.config(1)
+    src = np.asarray(m.obs_x[:2], dtype=np.float64)
+    g = Fmt2d(0).upload(m)
+    ref = None
+    for nt in (256, 384, 512):
+        g.set_solve_threads(nt).forward(src, (1, 3))
+        fs = [g.field(s, tf) for s in range(2) for tf in fields_of(phase_mask((1, 3)))]
+        if ref is None:
+            ref = fs
+            continue
+        for a, b in zip(ref, fs):
+            assert np.array_equal(a[0], b[0])
+            assert np.array_equal(a[1], b[1], equal_nan=True)
+    r = g.autotune(src, (1, 3))
+    assert r["threads"] in (256, 384, 512) and all(v > 0 for v in r["ms"].values())
+    T = g.field(1, 5)[0]
+    assert np.array_equal(T, ref[-1][0])
+    g.close()
