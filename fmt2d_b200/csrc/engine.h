@@ -167,7 +167,7 @@ class Engine {
   SolveLane lanes_[kChains];
   cudaEvent_t ev_start_ = nullptr;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
-      d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_;
+      d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_, d_sft_, d_sfjobs_;
   int npick_ = -1, rows_ = 0;
   long long nnz_ = 0;
   double trace_ms_ = 0.0;

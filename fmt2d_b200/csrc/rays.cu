@@ -641,8 +641,9 @@ __device__ void trace_section(RayState& R, int seqnum, double x_in, double z_in,
 }
 
 // inversion2d.f90:6344-6438: best seafloor entry point of an in-water pick.
-__device__ void optimal_entry(const TrModel& M, const TrRegion& r, const double* T, double rx,
-                              double rz, double& ex, double& ez, double& wt) {
+__device__ void optimal_entry(const TrModel& M, const TrRegion& r, const double* T,
+                              const double* sft, double rx, double rz, double& ex, double& ez,
+                              double& wt) {
   const int nsf = M.nx;
   const double* sz = M.ifz[2];
   const double* sxp = M.xpos;
@@ -658,9 +659,11 @@ __device__ void optimal_entry(const TrModel& M, const TrRegion& r, const double*
   double tbest = kHugeT;
   const double z0 = sf_z(rx);
   double xb = rx, zb = z0, wb = (z0 - rz) / M.vwater;
+  // the field's time at each seafloor node is the same for every pick of the
+  // source: precomputed once per field (sft), else interpolated here
   for (int i = 0; i < nsf; ++i) {
     const double xt = sxp[i], zs = sz[i];
-    const double tf = time_at(M, r, T, xt, zs);
+    const double tf = sft ? sft[i] : time_at(M, r, T, xt, zs);
     if (tf > kHugeT * 0.5) continue;
     const double tw = sqrt((xt - rx) * (xt - rx) + (zs - rz) * (zs - rz)) / M.vwater;
     if (tf + tw < tbest) { tbest = tf + tw; xb = xt; zb = zs; wb = tw; }
@@ -798,7 +801,7 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
         recx = pk.rx;
         recz = pk.rz;
       } else {
-        optimal_entry(M, lr, R.F[last_tf].T, pk.rx, pk.rz, recx, recz, wt);
+        optimal_entry(M, lr, R.F[last_tf].T, R.F[last_tf].sft, pk.rx, pk.rz, recx, recz, wt);
       }
     }
     // trace_ray_from_receiver2d
@@ -828,7 +831,19 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
   }
 }
 
+__global__ void k_sf_times(const TrModel* Mp, const SfJob* jobs, int njobs, int nx) {
+  const TrModel& M = *Mp;
+  const SfJob J = jobs[blockIdx.y];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
+    J.out[i] = time_at(M, M.reg[J.reg], J.T, M.xpos[i], M.ifz[2][i]);
+}
+
 }  // namespace
+
+void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStream_t st) {
+  if (njobs <= 0) return;
+  k_sf_times<<<dim3((nx + 127) / 128, njobs), 128, 0, st>>>(m, jobs, njobs, nx);
+}
 
 void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, const double* src_z,
                const TrPick* picks, int npick, double* t_calc, int* valid, unsigned* cnt,

@@ -37,7 +37,21 @@ struct TrPick {
 struct TrField {
   const double* T = nullptr;
   const double2* G = nullptr;
+  const double* sft = nullptr;    // the field's time at every seafloor node (the entry
+                                  // search's scan), for the terminal fields of phases 1-3
 };
+
+// One field whose seafloor-node times the entry search needs.
+struct SfJob {
+  const double* T = nullptr;
+  int reg = 0;
+  double* out = nullptr;          // nx values
+};
+
+// out[i] = the field's interpolated time at seafloor node i, for every job
+// (the same interpolation the entry search applies, done once per field
+// instead of once per pick).
+void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStream_t st);
 
 // Trace every pick.  Pass 1 (rows == nullptr): t_calc, valid and the number
 // of Frechet contributions of each pick (cnt).  Pass 2: the contributions

@@ -107,9 +107,39 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
         tf[(size_t)s * 13 + k].T = fields_[s][k].T.as<double>();
         tf[(size_t)s * 13 + k].G = fields_[s][k].Gout.as<double2>();
       }
+  // the entry search's seafloor-node times, once per terminal field of
+  // phases 1-3 (tf1, tf3, tf5) of every source
+  std::vector<SfJob> jobs;
+  {
+    const int nsf = m_.nx;
+    size_t nj = 0;
+    for (int s = 0; s < ns; ++s)
+      for (int k : {1, 3, 5})
+        if (fields_[s][k].solved) ++nj;
+    d_sft_.alloc(std::max<size_t>(nj, 1) * nsf * sizeof(double));
+    if (!d_sft_.p) return "device allocation failed (seafloor times)";
+    size_t j = 0;
+    for (int s = 0; s < ns; ++s)
+      for (int k : {1, 3, 5})
+        if (fields_[s][k].solved) {
+          SfJob J;
+          J.T = fields_[s][k].T.as<double>();
+          J.reg = kTf[k].reg;
+          J.out = d_sft_.as<double>() + j * nsf;
+          tf[(size_t)s * 13 + k].sft = J.out;
+          jobs.push_back(J);
+          ++j;
+        }
+  }
   std::string e;
   if (!(e = put_vec(d_picks_, pk.data(), (size_t)npick, stream_)).empty()) return e;
   if (!(e = put_vec(d_trfields_, tf.data(), tf.size(), stream_)).empty()) return e;
+  if (!jobs.empty()) {
+    if (!(e = put_vec(d_sfjobs_, jobs.data(), jobs.size(), stream_)).empty()) return e;
+    tr_sf_times(d_trmodel_.as<TrModel>(), d_sfjobs_.as<SfJob>(), (int)jobs.size(), m_.nx, stream_);
+    ++stats_.launches;
+    TCK(cudaGetLastError());
+  }
   if (!(e = put_vec(d_srcx_, src_x_.data(), (size_t)ns, stream_)).empty()) return e;
   if (!(e = put_vec(d_srcz_, src_z_.data(), (size_t)ns, stream_)).empty()) return e;
   const size_t np = (size_t)std::max(npick, 1);
