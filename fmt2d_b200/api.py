@@ -323,6 +323,19 @@ class Fmt2d:
         self._check(self.L.fmt2d_gtg_diag(self.h, N.ptr(out)), "fmt2d_gtg_diag")
         return out
 
+    def set_param_grid(self, coarse_idx=None, n_vel_parms=0, iface_nodes=0):
+        """The LSQR's parameter grid (fmt2d_set_param_grid): coarse_idx (nzc,
+        nxc) of fmt2d_projection with its velocity and interface parameter
+        counts, or None for the model's own numbering."""
+        if coarse_idx is None:
+            rc = self.L.fmt2d_set_param_grid(self.h, 0, 0, None, 0, 0)
+        else:
+            ci = np.ascontiguousarray(coarse_idx, dtype=np.int32)
+            rc = self.L.fmt2d_set_param_grid(self.h, ci.shape[1], ci.shape[0], N.ptr(ci),
+                                             int(n_vel_parms), int(iface_nodes))
+        self._check(rc, "fmt2d_set_param_grid")
+        return self
+
     def set_smoothing(self, mvscale, corr_x=0.0, corr_z=0.0, corr_x_iface=0.0):
         """Gaussian smoothing operators of the smooth_type 2/3 LSQR layouts
         (fmt2d_set_smoothing): R_h (corr_x > 0), R_v (corr_z > 0) and the

@@ -17,6 +17,8 @@ struct fmt2d_ctx {
   fmt2d::Model model;
   std::string err;
   bool has_model = false;
+  bool param_grid = false;              // the LSQR smooths on an explicit parameter grid
+  int param_count = 0;                  // its parameters
   bool need_gpu(int& code) {
     if (eng) return true;
     err = "host-only context (device -1): no GPU work possible";
@@ -81,6 +83,7 @@ int fmt2d_upload_model(fmt2d_ctx* ctx, const fmt2d_model_desc* d) {
     e = ctx->lsqr->set_geometry(ctx->model);
     if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
   }
+  ctx->param_grid = false;
   ctx->has_model = true;
   return FMT2D_OK;
 }
@@ -124,6 +127,7 @@ int fmt2d_update_model(fmt2d_ctx* ctx, const double* vel, const double* iface_z)
     e = ctx->lsqr->set_geometry(ctx->model);
     if (!e.empty()) return ctx->fail(FMT2D_ERR_CUDA, e);
   }
+  ctx->param_grid = false;
   ctx->has_model = true;
   return FMT2D_OK;
 }
@@ -397,6 +401,21 @@ int fmt2d_set_smoothing(fmt2d_ctx* ctx, double corr_x, double corr_z, double cor
   return FMT2D_OK;
 }
 
+int fmt2d_set_param_grid(fmt2d_ctx* ctx, int nxc, int nzc, const int* coarse_idx,
+                         int n_vel_parms, int iface_nodes) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  const std::string e =
+      coarse_idx ? ctx->lsqr->set_param_grid(nxc, nzc, coarse_idx, n_vel_parms, iface_nodes)
+                 : ctx->lsqr->set_geometry(ctx->model);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_ARG, e);
+  ctx->param_grid = coarse_idx != nullptr;
+  ctx->param_count = n_vel_parms + iface_nodes;
+  return FMT2D_OK;
+}
+
 int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residual,
                const double* gtg_diag, const double* dm_sum, double* dm, int* iters, double* rnorm,
                double* bnorm, double* test2) {
@@ -408,8 +427,8 @@ int fmt2d_lsqr(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double* residua
   if (p->smooth_type < 1 || p->smooth_type > 3)
     return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1, 2 or 3");
   if (p->max_iter < 1) return ctx->fail(FMT2D_ERR_ARG, "max_iter must be >= 1");
-  if (ctx->lsqr->nparm() != ctx->model.n_inv_parms)
-    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the model's inversion parameters");
+  if (ctx->lsqr->nparm() != (ctx->param_grid ? ctx->param_count : ctx->model.n_inv_parms))
+    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the inversion parameters");
   fmt2d::LsqrParams q;
   q.smooth_type = p->smooth_type;
   q.max_iter = p->max_iter;
@@ -438,8 +457,8 @@ int fmt2d_lsqr_noalloc(fmt2d_ctx* ctx, const fmt2d_lsqr_params* p, const double*
   if (ctx->lsqr->nparm() == 0) return ctx->fail(FMT2D_ERR_STATE, "no matrix set");
   if (p->smooth_type != 1) return ctx->fail(FMT2D_ERR_ARG, "smooth_type must be 1 (Laplacian)");
   if (p->max_iter < 1) return ctx->fail(FMT2D_ERR_ARG, "max_iter must be >= 1");
-  if (ctx->lsqr->nparm() != ctx->model.n_inv_parms)
-    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the model's inversion parameters");
+  if (ctx->lsqr->nparm() != (ctx->param_grid ? ctx->param_count : ctx->model.n_inv_parms))
+    return ctx->fail(FMT2D_ERR_STATE, "G columns differ from the inversion parameters");
   fmt2d::LsqrParams q;
   q.smooth_type = p->smooth_type;
   q.max_iter = p->max_iter;

@@ -618,15 +618,22 @@ Lsqr::~Lsqr() {
 }
 
 std::string Lsqr::set_geometry(const Model& m) {
-  const int nx = m.nx, nz = m.nz;
-  // a new model: the smoothing matrices of the last one no longer apply
+  return set_param_grid(m.nx, m.nz, m.inv_idx.data(), m.n_vel_parms,
+                        m.iface_inv > 0 ? m.nx : 0);
+}
+
+std::string Lsqr::set_param_grid(int nx, int nz, const int* idx, int nvp, int if_n) {
+  if (nx < 1 || nz < 1 || !idx || nvp < 0 || if_n < 0) return "bad parameter grid";
+  for (size_t k = 0; k < (size_t)nx * nz; ++k)
+    if (idx[k] < 0 || idx[k] > nvp) return "parameter grid ids must be 0..n_vel_parms";
+  // a new parameter grid: smoothing matrices built for another no longer apply
   for (bool& h : have_sm_) h = false;
   sm_np_ = -1;
-  nvp_ = m.n_vel_parms;
-  if_start_ = m.n_vel_parms;
-  if_n_ = m.iface_inv > 0 ? nx : 0;
+  nvp_ = nvp;
+  if_start_ = nvp;
+  if_n_ = if_n;
   std::vector<int4> nb((size_t)std::max(nvp_, 1), make_int4(-1, -1, -1, -1));
-  auto id = [&](int ix, int iz) { return m.inv_idx[(size_t)iz * nx + ix]; };
+  auto id = [&](int ix, int iz) { return idx[(size_t)iz * nx + ix]; };
   for (int iz = 0; iz < nz; ++iz)
     for (int ix = 0; ix < nx; ++ix) {
       const int k = id(ix, iz);

@@ -101,6 +101,10 @@ class Lsqr {
   ~Lsqr();
   // Laplacian neighbour table of the model's inversion numbering.
   std::string set_geometry(const Model& m);
+  // The same for an explicit parameter grid: idx[nz*nx] (ix fastest) holds
+  // 1-based velocity parameter ids (0: none), nvp of them, followed by if_n
+  // interface parameters (a coarse inversion grid, fmt2d_projection).
+  std::string set_param_grid(int nx, int nz, const int* idx, int nvp, int if_n);
   // Gaussian smoothing operators of the smooth_type 2/3 layouts
   // (build_gauss_smooth_matrix / build_iface_gauss_smooth_matrix with the
   // column scaling mvscale folded in): R_h if corr_x > 0, R_v if corr_z > 0,

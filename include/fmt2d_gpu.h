@@ -291,6 +291,17 @@ typedef struct fmt2d_lsqr_params {
 FMT2D_API int fmt2d_set_smoothing(fmt2d_ctx* ctx, double corr_x, double corr_z,
                                   double corr_x_iface, const double* mvscale);
 
+/* The parameter grid the LSQR's Laplacian smooths over, for inverting on a
+ * coarse grid (no reference counterpart: the reference inverts on the
+ * propagation grid): coarse_idx[nzc*nxc] (ix fastest) holds 1-based velocity
+ * parameter ids (0: none), n_vel_parms of them, followed by iface_nodes
+ * interface parameters, as fmt2d_projection returns them; G is then G P
+ * (fmt2d_project_rows) with n_vel_parms + iface_nodes columns.  coarse_idx
+ * NULL returns to the model's own numbering (also the state after every model
+ * upload or update).  smooth_type 1 only. */
+FMT2D_API int fmt2d_set_param_grid(fmt2d_ctx* ctx, int nxc, int nzc, const int* coarse_idx,
+                                   int n_vel_parms, int iface_nodes);
+
 /* LSQR on the current G: residual[ndata], gtg_diag[nparm] (NULL: computed
  * from G), dm_sum[nparm] (NULL: zeros) -> dm[nparm] and the reference's
  * lsqr_iter_out, rnorm_out, bnorm_out, test2_out (any may be NULL).  Needs an

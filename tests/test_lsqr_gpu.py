@@ -135,3 +135,38 @@ def test_lsqr_larger_random(oracle_lib):
     assert itg == ito
     assert np.abs(dmg - dmo).max() <= 1e-6 * np.abs(dmo).max()
     assert abs(rng_ - rno) <= 1e-9 * bng
+
+
+def test_lsqr_on_coarse_parameter_grid(oracle_lib, small):
+    """The device LSQR on a coarse inversion grid (fmt2d_set_param_grid with
+    fmt2d_projection's coarse_idx; G P from fmt2d_project_rows) against the
+    oracle's run_lsqr with the same explicit parameter grid: iterates within
+    1e-6 of max|dm| at 8 and 40 iterations; back on the model's grid the solve
+    is the model-grid solve again."""
+    from fmt2d_b200.api import project_rows
+    m, o, g, nd, npar, nvp, rp, gi, gv = small
+    pr = g.projection(4, 2, 4)
+    prp, pcol, pval = pr["P"]
+    npc, nvpc = pr["npar"], pr["nvp"]
+    crp, cgi, cgv = project_rows(rp, gi, gv, npar, prp, pcol, pval)
+    Gc = csr_to_scipy(nd, npc, crp, cgi, cgv)
+    gtg = np.asarray(Gc.multiply(Gc).sum(axis=0)).ravel()
+    rng = np.random.default_rng(31)
+    r = rng.normal(0.0, 0.05, nd)
+    dm_sum = rng.normal(0.0, 0.01, npc)
+    eps_min = max(1e-6, 1e-4 * gtg.max())
+    g.set_param_grid(pr["coarse_idx"], nvpc, npc - nvpc)
+    g.set_frechet(nd, npc, crp, cgi, cgv)
+    try:
+        for it in (8, 40):
+            dmo, ito, rno, _ = oracle_lib.lsqr_geom(pr["coarse_idx"], nvpc, npc - nvpc, nd, npc,
+                                                    cgi, cgv, crp, r, gtg, dm_sum, eps_min, 0.5,
+                                                    0.5, 3.0, 3.0, it)
+            dmg, itg, rng_, bng, _ = g.lsqr(r, dm_sum, gtg, wdv=0.5, wdv_iface=0.5, w_smooth=3.0,
+                                            w_smooth_iface=3.0, eps_min=eps_min, max_iter=it)
+            assert itg == ito
+            assert np.abs(dmg - dmo).max() <= 1e-6 * np.abs(dmo).max()
+            assert abs(rng_ - rno) <= 1e-9 * bng
+    finally:
+        g.set_param_grid(None)
+        g.set_frechet(nd, npar, rp, gi, gv)

@@ -6,8 +6,9 @@ compute_frechet_for_ray2d.
 Both sides trace on the same time fields (the device's, loaded into the
 oracle), so the comparison isolates the tracer: identical valid flags,
 receiver times within 1e-9 s, identical row index sets (bit-exact
-parameter indexing) and Frechet values within 1e-4 relative (north-star
-tolerance; the two differ only in summation order).  End to end (each side
+parameter indexing) and every Frechet value within 1e-4 relative (north-star
+tolerance; the two differ only in summation order), with an absolute floor
+of 1e-6 grid steps of path length.  End to end (each side
 on its own fields) receiver times must agree within 0.5 ms.
 """
 import numpy as np
@@ -60,8 +61,12 @@ def test_trace_and_rows_on_same_fields(oracle_lib, phases):
         np.testing.assert_array_equal(idx, r["idx"])
         n_rows += idx.size > 0
         if idx.size:   # a ray that stays in the water has no rows
-            scale = np.abs(r["val"]).max()
-            assert np.abs(val - r["val"]).max() <= 1e-4 * scale
+            # per entry: 1e-4 relative, with an absolute floor of 1e-6 grid
+            # steps of path length (entries are path length times bilinear
+            # weights; the two sides add the same contributions in a
+            # different order)
+            err = np.abs(val - r["val"])
+            assert np.all(err <= 1e-4 * np.abs(r["val"]) + 1e-6 * m.dx), err.max()
     assert n_rows >= 0.5 * len(pk)
     # end to end (the oracle on its own fields, traced before the fields were
     # replaced).  Valid flags can differ where a ray passes a grid node that
