@@ -286,6 +286,15 @@ class Fmt2d:
         self.npick, self.frechet_nnz = n, nnz.value
         return t, v.astype(bool), nnz.value
 
+    def trace_entries(self):
+        """Per pick of the last trace (fmt2d_trace_entries): water time, entry
+        x, entry z (the seafloor entry point of an in-water pick of phases
+        1-3, else the receiver)."""
+        wt, ex, ez = np.zeros(self.npick), np.zeros(self.npick), np.zeros(self.npick)
+        self._check(self.L.fmt2d_trace_entries(self.h, N.ptr(wt), N.ptr(ex), N.ptr(ez)),
+                    "fmt2d_trace_entries")
+        return wt, ex, ez
+
     def frechet_rows(self, index_base: int = 1):
         """CSR (row_ptr, gindx, gval) of the last trace (fmt2d_frechet_rows)."""
         rp = np.zeros(self.npick + 1, np.int32)

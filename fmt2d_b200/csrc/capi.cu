@@ -357,6 +357,15 @@ int fmt2d_frechet_rows(fmt2d_ctx* ctx, int* row_ptr, int* gindx, double* gval, i
   return FMT2D_OK;
 }
 
+int fmt2d_trace_entries(fmt2d_ctx* ctx, double* water_time, double* entry_x, double* entry_z) {
+  if (!ctx) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  const std::string e = ctx->eng->trace_entries(water_time, entry_x, entry_z);
+  if (!e.empty()) return ctx->fail(FMT2D_ERR_STATE, e);
+  return FMT2D_OK;
+}
+
 int fmt2d_set_frechet(fmt2d_ctx* ctx, int ndata, int nparm, const int* row_ptr,
                       const int* gindx, const double* gval, int index_base) {
   if (!ctx || !row_ptr || ndata < 0 || nparm <= 0 || (index_base != 0 && index_base != 1))

@@ -126,6 +126,9 @@ class Engine {
   std::string trace(const int* src, const int* phase, const double* rx, const double* rz,
                     int npick, double* t_calc, int* valid, long long* nnz);
   std::string frechet_rows(int* row_ptr, int* col, double* val, int base);
+  // per pick of the last trace: the ray's receiver end (seafloor entry point
+  // of an in-water pick of phases 1-3, else the receiver) and the water time
+  std::string trace_entries(double* water_time, double* entry_x, double* entry_z);
   double trace_ms() const { return trace_ms_; }
   long long frechet_nnz() const { return nnz_; }
   const Model& model() const { return m_; }
@@ -167,7 +170,8 @@ class Engine {
   SolveLane lanes_[kChains];
   cudaEvent_t ev_start_ = nullptr;
   DevBuf d_pvel_, d_invidx_, d_xpos_, d_trmodel_, d_picks_, d_trfields_, d_srcx_, d_srcz_,
-      d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_, d_sft_, d_sfjobs_;
+      d_tcalc_, d_valid_, d_cnt_, d_off_, d_rowptr_, d_tmp_, d_col_, d_val_, d_sft_, d_sfjobs_,
+      d_entry_;
   int npick_ = -1, rows_ = 0;
   long long nnz_ = 0;
   double trace_ms_ = 0.0;

@@ -753,7 +753,8 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
                                                const TrPick* picks, int npick, double* t_calc,
                                                int* valid, unsigned* cnt,
                                                const unsigned long long* off,
-                                               unsigned long long* keys, double* vals) {
+                                               unsigned long long* keys, double* vals,
+                                               double* entry) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npick) return;
   const TrModel& M = *Mp;
@@ -789,6 +790,7 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
     if (!R.F[rs.tf].T) ok = false;   // field not solved
   }
   double tr = kHugeT;
+  double ent_x = pk.rx, ent_z = pk.rz, ent_w = 0.0;   // the ray's receiver end, water time
   if (ok) {
     // invert2d_main.f90:517-537: a receiver above the seafloor is in water
     const double zsf = seafloor_z(M, pk.rx);
@@ -804,6 +806,9 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
         optimal_entry(M, lr, R.F[last_tf].T, R.F[last_tf].sft, pk.rx, pk.rz, recx, recz, wt);
       }
     }
+    ent_x = recx;
+    ent_z = recz;
+    ent_w = wt;
     // trace_ray_from_receiver2d
     tr = time_at(M, lr, R.F[last_tf].T, recx, recz);
     double rgx, rgz;
@@ -828,6 +833,11 @@ __global__ void __launch_bounds__(128) k_trace(const TrModel* Mp, const TrField*
     t_calc[p] = tr;
     valid[p] = ok ? 1 : 0;
     cnt[p] = ok ? sk.n : 0u;
+    if (entry) {
+      entry[3 * (size_t)p] = ent_x;
+      entry[3 * (size_t)p + 1] = ent_z;
+      entry[3 * (size_t)p + 2] = ent_w;
+    }
   }
 }
 
@@ -848,9 +858,9 @@ void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStr
 void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, const double* src_z,
                const TrPick* picks, int npick, double* t_calc, int* valid, unsigned* cnt,
                const unsigned long long* off, unsigned long long* keys, double* vals,
-               cudaStream_t st) {
+               double* entry, cudaStream_t st) {
   k_trace<<<(npick + 127) / 128, 128, 0, st>>>(m, fields, src_x, src_z, picks, npick, t_calc,
-                                               valid, cnt, off, keys, vals);
+                                               valid, cnt, off, keys, vals, entry);
 }
 
 }  // namespace fmt2d

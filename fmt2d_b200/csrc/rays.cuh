@@ -56,9 +56,12 @@ void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStr
 // Trace every pick.  Pass 1 (rows == nullptr): t_calc, valid and the number
 // of Frechet contributions of each pick (cnt).  Pass 2: the contributions
 // themselves at off[pick] (keys = pick << 32 | parameter id, 1-based).
+// entry (pass 1, may be null): per pick the receiver end of the ray (the
+// seafloor entry point of an in-water pick of phases 1-3, else the receiver)
+// and the water leg's time, 3 doubles.
 void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, const double* src_z,
                const TrPick* picks, int npick, double* t_calc, int* valid, unsigned* cnt,
                const unsigned long long* off, unsigned long long* keys, double* vals,
-               cudaStream_t st);
+               double* entry, cudaStream_t st);
 
 }  // namespace fmt2d

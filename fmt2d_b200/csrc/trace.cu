@@ -148,7 +148,8 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
   d_cnt_.alloc((np + 1) * sizeof(unsigned));
   d_off_.alloc((np + 1) * sizeof(unsigned long long));
   d_rowptr_.alloc((np + 1) * sizeof(int));
-  if (!d_tcalc_.p || !d_valid_.p || !d_cnt_.p || !d_off_.p || !d_rowptr_.p)
+  d_entry_.alloc(np * 3 * sizeof(double));
+  if (!d_tcalc_.p || !d_valid_.p || !d_cnt_.p || !d_off_.p || !d_rowptr_.p || !d_entry_.p)
     return "device allocation failed (picks)";
   // the timing events are released on every return
   struct Events {
@@ -169,7 +170,7 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
     TCK(cudaMemsetAsync(cnt, 0, (np + 1) * sizeof(unsigned), stream_));
     tr_launch(M, d_trfields_.as<TrField>(), d_srcx_.as<double>(), d_srcz_.as<double>(),
               d_picks_.as<TrPick>(), npick, d_tcalc_.as<double>(), d_valid_.as<int>(), cnt,
-              nullptr, nullptr, nullptr, stream_);
+              nullptr, nullptr, nullptr, d_entry_.as<double>(), stream_);
     ++stats_.launches;
     TCK(cudaGetLastError());
     // offsets of each pick's contributions (64-bit: long rays times many picks)
@@ -191,7 +192,7 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
     if (!keys.p || !vals.p || !keys2.p || !vals2.p) return "device allocation failed (Frechet)";
     tr_launch(M, d_trfields_.as<TrField>(), d_srcx_.as<double>(), d_srcz_.as<double>(),
               d_picks_.as<TrPick>(), npick, d_tcalc_.as<double>(), d_valid_.as<int>(), cnt, off,
-              keys.as<unsigned long long>(), vals.as<double>(), stream_);
+              keys.as<unsigned long long>(), vals.as<double>(), nullptr, stream_);
     ++stats_.launches;
     TCK(cudaGetLastError());
     const int n = (int)total;
@@ -269,6 +270,22 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
   trace_ms_ = ms;
   npick_ = npick;
   if (nnz) *nnz = nnz_;
+  return std::string();
+}
+
+std::string Engine::trace_entries(double* water_time, double* entry_x, double* entry_z) {
+  cudaSetDevice(device_);
+  if (npick_ < 0) return "no completed trace";
+  if (npick_ == 0) return std::string();
+  std::vector<double> e((size_t)npick_ * 3);
+  TCK(cudaMemcpyAsync(e.data(), d_entry_.p, e.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                      stream_));
+  TCK(cudaStreamSynchronize(stream_));
+  for (int p = 0; p < npick_; ++p) {
+    if (entry_x) entry_x[p] = e[3 * (size_t)p];
+    if (entry_z) entry_z[p] = e[3 * (size_t)p + 1];
+    if (water_time) water_time[p] = e[3 * (size_t)p + 2];
+  }
   return std::string();
 }
 

@@ -243,3 +243,31 @@ def _es14_6(x: float) -> str:
     """Fortran ES14.6: d.dddddde+xx right-justified in 14 columns."""
     m, e = f"{x:.6e}".split("e")
     return f"{m}E{int(e):+03d}".rjust(14)
+
+
+def write_arrivals(arrivals_path: str, obs_path: str, entry_path: str, ircv, src, phase,
+                   t_calc, valid, water_time, entry_x, entry_z):
+    """write_arrivals2d (fmt2d_main.f90:1655-1719): the arrivals file (every
+    ray: receiver, source, phase, arrival time, time without the water leg,
+    water time; -1 for an invalid ray), the observed-times file (the valid
+    rays, their count first) and entry_points.dat (the valid rays' seafloor
+    entry points and water times, their count first).  Receivers and sources
+    are written 1-based; ircv is the pick's receiver (shot) index, 0-based.
+    The reference writes one entry point per receiver and phase (the last
+    source's); this writes each ray's own."""
+    valid = np.asarray(valid, dtype=bool)
+    n = int(valid.sum())
+    with open(arrivals_path, "w") as fa, open(obs_path, "w") as fo, open(entry_path, "w") as fe:
+        fo.write(f"{n}\n")
+        fe.write(f"{n}\n")
+        for i in range(len(valid)):
+            head = f"{int(ircv[i]) + 1:8d}{int(src[i]) + 1:8d}{int(phase[i]):8d}"
+            w = float(water_time[i])
+            if valid[i]:
+                t = float(t_calc[i])
+                fa.write(f"{head}{t:15.6f}{t - w:15.6f}{w:12.6f}\n")
+                fo.write(f"{head}{t:15.6f}\n")
+                fe.write(f"{head}{float(entry_x[i]):15.6f}{float(entry_z[i]):15.6f}{w:12.6f}\n")
+            else:
+                fa.write(f"{head}{-1.0:15.6f}{-1.0:15.6f}{w:12.6f}\n")
+    return n

@@ -241,6 +241,14 @@ FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
 FMT2D_API int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
                           const double* rz, int npick, double* t_calc, int* valid,
                           long long* nnz);
+/* Per pick of the last fmt2d_trace (npick values each, any may be NULL): the
+ * water leg's time (ray%water_time, 0 for a receiver below the seafloor or a
+ * Pg_ss / Pg_ss2 pick) and the ray's receiver end (the seafloor entry point
+ * find_optimal_entry_inv chose, src/inversion2d.f90:6344-6438, else the
+ * receiver): what write_arrivals2d and entry_points.dat report
+ * (fmt2d_main.f90:1655-1719). */
+FMT2D_API int fmt2d_trace_entries(fmt2d_ctx* ctx, double* water_time, double* entry_x,
+                                  double* entry_z);
 /* The Frechet rows of the last fmt2d_trace as CSR over all its picks (an
  * invalid pick's row is empty): row_ptr[npick+1], gindx[nnz] parameter ids in
  * ascending order (the inversion numbering of fmt2d_inv_index, interface

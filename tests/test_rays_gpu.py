@@ -40,6 +40,7 @@ def test_trace_and_rows_on_same_fields(oracle_lib, phases):
     pk = m.picks
     src, ph = pk[:, 0].astype(np.int32), pk[:, 1].astype(np.int32)
     t, valid, nnz = g.trace(src, ph, pk[:, 2], pk[:, 3])
+    wt, ex, ez = g.trace_entries()
     assert len(pk) > 0
     own = [o.trace(int(p[0]), int(p[1]), p[2], p[3]) for p in pk]
     # same fields: load the device fields into the oracle
@@ -58,6 +59,12 @@ def test_trace_and_rows_on_same_fields(oracle_lib, phases):
             assert idx.size == 0
             continue
         assert abs(t[i] - r["t"]) <= 1e-9, (i, t[i], r["t"])
+        # the ray's receiver end (the seafloor entry point of an in-water
+        # pick) is a point of the oracle's ray; the water leg runs from the
+        # receiver to it at the water velocity
+        assert np.hypot(r["pts"][:, 0] - ex[i], r["pts"][:, 1] - ez[i]).min() <= 1e-9
+        leg = np.hypot(ex[i] - p[2], ez[i] - p[3]) / m.vwater if wt[i] > 0.0 else 0.0
+        assert abs(wt[i] - leg) <= 1e-12
         np.testing.assert_array_equal(idx, r["idx"])
         n_rows += idx.size > 0
         if idx.size:   # a ray that stays in the water has no rows

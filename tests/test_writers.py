@@ -59,3 +59,16 @@ def test_residual_lines(tmp_path):
     lines = open(p).read().splitlines()
     assert n == 1 and len(lines) == 2
     assert lines[1] == "     1      10.500     0.005   1    2.500000    2.400000  1.000000E-01"
+
+
+def test_arrival_files(tmp_path):
+    a, o, e = (str(tmp_path / f) for f in ("arrivals.dat", "obs.dat", "entry_points.dat"))
+    n = io.write_arrivals(a, o, e, [0, 4], [2, 2], [1, 3], [3.25, 7.0], [True, False],
+                          [0.5, 0.25], [10.0, 0.0], [3.5, 0.0])
+    assert n == 1
+    assert open(a).read().splitlines() == [
+        "       1       3       1       3.250000       2.750000    0.500000",
+        "       5       3       3      -1.000000      -1.000000    0.250000"]
+    assert open(o).read().splitlines() == ["1", "       1       3       1       3.250000"]
+    assert open(e).read().splitlines() == [
+        "1", "       1       3       1      10.000000       3.500000    0.500000"]
