@@ -129,8 +129,11 @@ void define_region(Model& m, Region& r, int itop, int ibot) {
   r.tiles_y = (r.H + kTileH - 1) / kTileH;
   r.pitch = r.tiles_x * kTileW;
   r.slot_of_node.assign(r.nnode, 0);
-  for (int ix = 0; ix < nx; ++ix)
-    for (int iz = r.r0[ix]; iz <= r.r1[ix]; ++iz) {
+  // node ids run down each column (the reference's order); the grid tables
+  // are written row by row (row-major arrays)
+  for (int iz = zlo; iz <= zhi; ++iz)
+    for (int ix = 0; ix < nx; ++ix) {
+      if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
       const size_t gi = m.g(ix, iz);
       const int id = r.col_base[ix] + (iz - r.r0[ix]);
       r.slot_of_node[id] = r.slot_grid(ix, iz);
@@ -166,8 +169,11 @@ void finish_region(Model& m, Region& r) {
   const Interface& fb = m.ifc[r.ibot];
   const uint8_t tbit = (uint8_t)(1u << r.itop), bbit = (uint8_t)(1u << r.ibot);
   auto cut = [&](int cx, int cz) { return m.cell_cut[(size_t)cz * nx + cx]; };
-  for (int ix = 0; ix < nx; ++ix) {
-    for (int iz = r.r0[ix]; iz <= r.r1[ix]; ++iz) {
+  // rows outer, columns inner: every per-node array is row-major, and each
+  // slot's code and velocity depend on nothing computed here
+  for (int iz = r.z_lo; iz <= r.z_hi; ++iz) {
+    for (int ix = 0; ix < nx; ++ix) {
+      if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
       const int s = r.slot_grid(ix, iz);
       double v = m.vel[m.g(ix, iz)];
       if (iz < m.nz - 1 && !in_region(r, ix, iz + 1)) {
@@ -243,24 +249,38 @@ std::string build_model(Model& m, int nx, int nzs, const double* xpos, const dou
   m.nz = (int)std::lround(zmax / dx) + 1;
   const int nz = m.nz;
   m.vel.assign((size_t)nx * nz, 0.0);
+  // the seafloor depth of every column
+  std::vector<double> zsf(nx);
   for (int ix = 0; ix < nx; ++ix) {
     const int iv = std::min(ix, nx - 2);
     const double wx = std::min(1.0, std::max(0.0, double(ix - iv)));
-    const double zsf = (1.0 - wx) * topo[iv] + wx * topo[iv + 1];
-    for (int iz = 0; iz < nz; ++iz) {
-      const double pz = grid_z(m, iz) - zsf;
+    zsf[ix] = (1.0 - wx) * topo[iv] + wx * topo[iv + 1];
+  }
+  // With zrel non-decreasing, the smesh row that brackets a node is unique
+  // and never moves up a column (pz grows down it): each column's search
+  // resumes at the row the node above found, with the same result as a
+  // search from the top.  Otherwise every search starts at the top.
+  bool monotone = true;
+  for (int io = 0; io + 1 < nzs; ++io) monotone = monotone && zrel[io] <= zrel[io + 1];
+  std::vector<int> from(nx, 0);
+  // rows outer: m.vel is row-major
+  for (int iz = 0; iz < nz; ++iz) {
+    double* vrow = &m.vel[m.g(0, iz)];
+    for (int ix = 0; ix < nx; ++ix) {
+      const double pz = grid_z(m, iz) - zsf[ix];
       double v;
       if (pz < 0.0) v = vwater;
       else if (pz >= zrel[nzs - 1]) v = vel[(size_t)(nzs - 1) * nx + ix];
       else {
-        int io = 0;
-        for (io = 0; io < nzs - 1; ++io)
+        int io = monotone ? from[ix] : 0;
+        for (; io < nzs - 1; ++io)
           if (pz >= zrel[io] && pz < zrel[io + 1]) break;
-        if (io >= nzs - 1) io = nzs - 2;
+        if (io >= nzs - 1) io = nzs - 2;   // no bracketing row
+        else if (monotone) from[ix] = io;
         const double wz = (pz - zrel[io]) / (zrel[io + 1] - zrel[io]);
         v = (1.0 - wz) * vel[(size_t)io * nx + ix] + wz * vel[(size_t)(io + 1) * nx + ix];
       }
-      m.vel[m.g(ix, iz)] = v;
+      vrow[ix] = v;
     }
   }
   m.zbot = zrel[nzs - 1] + maxtopo;
