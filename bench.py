@@ -24,6 +24,8 @@ eikonal time fields, solved through the library's public entry point.
 * rays, lsqr: ray backtrace + Frechet rows of every Pg and PmP pick of the
            model (picks/s, device-timed), and the LSQR solve on those rows
            (s per LSQR iteration).
+* adjoint: the misfit gradient w.r.t. the grid slowness by the discrete
+           adjoint of the same fields (fmt2d_misfit_gradient, s per gradient).
 * cpu_baseline: the FP64 CPU restatement of the reference algorithm (oracle/)
            on the host cores, over a bounded sample of the same workload
            (pool warmed first, median of 3 timed repetitions).
@@ -358,7 +360,21 @@ def rays_and_lsqr(g, m, stream):
             "iterations": int(it), "ndata": int(nd), "nparm": int(npar), "nnz": int(sgi.size),
             "ms": round(ls["ms"], 3), "smooth_type": 1,
             "note": "fmt2d_lsqr, damping 1, Laplacian 10, device-timed"}
-    return rays, lsqr
+    # misfit gradient w.r.t. the grid slowness by the discrete adjoint of the
+    # same fields (the call traces the picks again), wall time of the call
+    g.misfit_gradient(src, ph, rx, rz, obs, 0.040)       # warm
+    t0 = time.perf_counter()
+    out = g.misfit_gradient(src, ph, rx, rz, obs, 0.040)
+    adj_s = time.perf_counter() - t0
+    info = out["info"]
+    if np.any(info[:3] != 0):
+        raise RuntimeError(f"adjoint could not follow the forward: {info[:3].tolist()}")
+    adjoint = {"value": round(adj_s, 4), "unit": "s per misfit gradient",
+               "fields": int(info[4]), "nodes": int(info[5]), "sweep_rounds": int(info[3]),
+               "picks": int(P.shape[0]),
+               "note": "fmt2d_misfit_gradient: trace + discrete adjoint of every field + map "
+                       "onto the 2001x401 slowness grid, wall time, fields resident"}
+    return rays, lsqr, adjoint
 
 
 def inversion_iterations(local, n_iter: int = 2, cfg: int = 1):
@@ -556,9 +572,9 @@ def run_ours(args, world, rank, local):
     # same steps, outside the timed region)
     try:
         g.forward(src, PHASES)
-        rays, lsqr = rays_and_lsqr(g, m, stream)
+        rays, lsqr, adjoint = rays_and_lsqr(g, m, stream)
     except Exception as ex:  # the eikonal line is the result; report why these are absent
-        rays = lsqr = {"unavailable": str(ex)[:200]}
+        rays = lsqr = adjoint = {"unavailable": str(ex)[:200]}
 
     # ---- s per inversion iteration (rank 0 of a 1-GPU run; outside the
     # timed region)
@@ -618,7 +634,7 @@ def run_ours(args, world, rank, local):
                         "bytes_per_node": 16, "fp64_bytes_per_node": 36,
                         "fp64_frac": round(36.0 * nodes_step / (step_ms / 1e3) / 1e9 / peak, 7)},
            "solver": solver, "autotune": tune,
-           "rays": rays, "lsqr": lsqr, "inversion": inversion, "uneven_batch": batch,
+           "rays": rays, "lsqr": lsqr, "adjoint": adjoint, "inversion": inversion, "uneven_batch": batch,
            "plain": plain,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "cpu_baseline": cpu}

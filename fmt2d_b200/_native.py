@@ -119,6 +119,10 @@ def lib():
     L.fmt2d_set_solve_threads.argtypes = [V, C.c_int]
     L.fmt2d_set_param_grid.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
     L.fmt2d_trace_entries.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fmt2d_misfit_gradient.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_int, P(C.c_double),
+                                        C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_autotune.argtypes = [V, _dp, C.c_int, C.c_int, P(C.c_int), C.c_void_p]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int

@@ -117,6 +117,7 @@ class Fmt2d:
         self.h = h
         self.device = device
         self._keep = None
+        self.npick, self.frechet_nnz = 0, None
 
     def close(self):
         if getattr(self, "h", None):
@@ -286,6 +287,38 @@ class Fmt2d:
         self.npick, self.frechet_nnz = n, nnz.value
         return t, v.astype(bool), nnz.value
 
+    def misfit_gradient(self, src, phase, rx, rz, t_obs, sigma, want=("slow",)):
+        """Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks
+        (phases 1-3; t_obs < 0: no pick) on the last forward's fields and its
+        gradient by the discrete adjoint of the fields
+        (fmt2d_misfit_gradient).  Returns a dict: misfit, t_calc, valid,
+        grad_slow and / or grad_vel ((nz, nx), as `want` asks), info (the
+        adjoint's counters, see the header)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        phase = np.ascontiguousarray(phase, dtype=np.int32)
+        rx = np.ascontiguousarray(rx, dtype=np.float64)
+        rz = np.ascontiguousarray(rz, dtype=np.float64)
+        t_obs = np.ascontiguousarray(t_obs, dtype=np.float64)
+        sigma = np.broadcast_to(np.asarray(sigma, dtype=np.float64), src.shape).copy()
+        n = src.size
+        t = np.zeros(n)
+        v = np.zeros(n, np.int32)
+        J = C.c_double()
+        gs = np.zeros(self.nx * self.nz) if "slow" in want else None
+        gvel = np.zeros(self.nx * self.nz) if "vel" in want else None
+        info = np.zeros(8)
+        self._check(self.L.fmt2d_misfit_gradient(
+            self.h, N.ptr(src), N.ptr(phase), N.ptr(rx), N.ptr(rz), N.ptr(t_obs), N.ptr(sigma), n,
+            C.byref(J), N.ptr(t), N.ptr(v), N.ptr(gs), N.ptr(gvel), N.ptr(info)),
+            "fmt2d_misfit_gradient")
+        self.npick, self.frechet_nnz = n, None
+        out = {"misfit": J.value, "t_calc": t, "valid": v.astype(bool), "info": info}
+        if gs is not None:
+            out["grad_slow"] = gs.reshape(self.nz, self.nx)
+        if gvel is not None:
+            out["grad_vel"] = gvel.reshape(self.nz, self.nx)
+        return out
+
     def trace_entries(self):
         """Per pick of the last trace (fmt2d_trace_entries): water time, entry
         x, entry z (the seafloor entry point of an in-water pick of phases
@@ -297,6 +330,9 @@ class Fmt2d:
 
     def frechet_rows(self, index_base: int = 1):
         """CSR (row_ptr, gindx, gval) of the last trace (fmt2d_frechet_rows)."""
+        if self.frechet_nnz is None:
+            raise RuntimeError("Frechet rows: call trace() first (misfit_gradient traces the "
+                               "picks but does not report the row count)")
         rp = np.zeros(self.npick + 1, np.int32)
         gi = np.zeros(max(self.frechet_nnz, 1), np.int32)
         gv = np.zeros(max(self.frechet_nnz, 1))

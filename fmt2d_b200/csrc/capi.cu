@@ -346,6 +346,37 @@ int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, const double* 
   return FMT2D_OK;
 }
 
+int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
+                          const double* rz, const double* t_obs, const double* sigma, int npick,
+                          double* misfit, double* t_calc, int* valid, double* grad_slow,
+                          double* grad_vel, double* info) {
+  if (!ctx || !misfit || npick < 0 ||
+      (npick > 0 && (!src || !phase || !rx || !rz || !t_obs || !sigma || !t_calc || !valid)))
+    return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  if (ctx->eng->nsrc() == 0) return ctx->fail(FMT2D_ERR_STATE, "no forward solved");
+  const fmt2d::Model& m = ctx->eng->model();
+  const size_t nn = (size_t)m.nx * m.nz;
+  std::vector<double> gv((grad_slow || grad_vel) ? nn : 0);
+  const std::string e = ctx->eng->misfit_gradient(src, phase, rx, rz, t_obs, sigma, npick, misfit,
+                                                  t_calc, valid, gv.empty() ? nullptr : gv.data(),
+                                                  info);
+  if (!e.empty()) {
+    const bool arg = e.find("range") != std::string::npos || e.find("phases") != std::string::npos ||
+                     e.find("sigma") != std::string::npos;
+    const bool state = e.find("not solved") != std::string::npos ||
+                       e.find("missing") != std::string::npos;
+    return ctx->fail(arg ? FMT2D_ERR_ARG : state ? FMT2D_ERR_STATE : FMT2D_ERR_CUDA, e);
+  }
+  if (grad_vel) std::copy(gv.begin(), gv.end(), grad_vel);
+  // s = 1/v: dJ/ds = -v^2 dJ/dv
+  if (grad_slow)
+    for (size_t i = 0; i < nn; ++i) grad_slow[i] = -(m.vel[i] * m.vel[i]) * gv[i];
+  return FMT2D_OK;
+}
+
 int fmt2d_frechet_rows(fmt2d_ctx* ctx, int* row_ptr, int* gindx, double* gval, int index_base) {
   if (!ctx || (index_base != 0 && index_base != 1)) return FMT2D_ERR_ARG;
   int code = 0;

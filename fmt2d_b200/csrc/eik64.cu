@@ -617,13 +617,18 @@ __global__ void k_water_fix(Fld64* fields, const int* upward, int nf) {
 
 // PmP head-wave min-plus sweep along the Moho (inversion2d.f90:4294-4409), one
 // field per thread; node table and velocities are precomputed per model.
+// The solved times the sweep replaces are saved first (pre, nx per field:
+// the adjoint re-derives each node's winning update from them).
 __global__ void k_headwave(Fld64* fields, const int* hw_slot, const double* hw_v, double dx_if,
-                           int nx, double* scratch, const int* which, int nsel) {
+                           int nx, double* scratch, const int* which, int nsel,
+                           double* const* pre) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsel) return;
   Fld64& F = fields[which[q]];
   double* th = scratch + (size_t)q * nx;
   for (int n = 0; n < nx; ++n) th[n] = hw_slot[n] >= 0 ? F.T[hw_slot[n]] : kHugeD;
+  if (pre && pre[q])
+    for (int n = 0; n < nx; ++n) pre[q][n] = th[n];
   for (int n = 1; n < nx; ++n)
     if (hw_v[n] > 0.0) th[n] = fmin(th[n], th[n - 1] + dx_if / hw_v[n]);
   for (int n = nx - 2; n >= 0; --n)
@@ -765,8 +770,9 @@ void e64_finish(Fld64* f, int nf, size_t max_slots, const int* water_up, cudaStr
   k_water_fix<<<dim3(64, nf), 128, 0, st>>>(f, water_up, nf);
 }
 void e64_headwave(Fld64* f, const int* hw_slot, const double* hw_v, double dx_if, int nx,
-                  double* scratch, const int* which, int nsel, cudaStream_t st) {
-  k_headwave<<<(nsel + 31) / 32, 32, 0, st>>>(f, hw_slot, hw_v, dx_if, nx, scratch, which, nsel);
+                  double* scratch, const int* which, int nsel, double* const* pre,
+                  cudaStream_t st) {
+  k_headwave<<<(nsel + 31) / 32, 32, 0, st>>>(f, hw_slot, hw_v, dx_if, nx, scratch, which, nsel, pre);
 }
 void e64_export(const double* T, const double2* G, const int* slot_of_node, int nnode, double* oT,
                 double* ogx, double* ogz, cudaStream_t st) {

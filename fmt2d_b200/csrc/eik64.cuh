@@ -108,8 +108,12 @@ int e64_tiles_max();
 // is listed in list_in and counted in cnt[1].
 void e64_verify(Fld64* f, int nf, size_t max_slots, cudaStream_t st);
 void e64_finish(Fld64* f, int nf, size_t max_slots, const int* water_up, cudaStream_t st);
+// PmP head-wave sweep of the selected fields; pre (device array of nsel
+// pointers, may be null, entries may be null) receives each field's solved
+// times at the nx sweep nodes before the sweep lowers them.
 void e64_headwave(Fld64* f, const int* hw_slot, const double* hw_v, double dx_if, int nx,
-                  double* scratch, const int* which, int nsel, cudaStream_t st);
+                  double* scratch, const int* which, int nsel, double* const* pre,
+                  cudaStream_t st);
 void e64_export(const double* T, const double2* G, const int* slot_of_node, int nnode, double* oT,
                 double* ogx, double* ogz, cudaStream_t st);
 

@@ -32,10 +32,15 @@
 #include "eik64.cuh"
 #include "model.h"
 
+// A second translation unit that includes this header defines FMT_HD_LINK as
+// `static` so the two copies of these functions do not collide at link time.
+#ifndef FMT_HD_LINK
+#define FMT_HD_LINK
+#endif
 #if defined(__CUDACC__)
-#define FMT_HD __host__ __device__
+#define FMT_HD FMT_HD_LINK __host__ __device__
 #else
-#define FMT_HD
+#define FMT_HD FMT_HD_LINK
 #endif
 
 #ifdef __CUDA_ARCH__

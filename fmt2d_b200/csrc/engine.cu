@@ -200,7 +200,7 @@ std::string Engine::upload(const Model& m) {
   {
     const Region& R6 = m.reg[6];
     const Interface& moho = m.ifc[4];
-    std::vector<int> hs(m.nx, -1);
+    std::vector<int> hs(m.nx, -1), hvs(m.nx, -1);   // sweep node; slot whose velocity hv is
     std::vector<double> hv(m.nx, 0.0);
     for (int n = 0; n < m.nx; ++n) {
       int id = 0;
@@ -220,15 +220,20 @@ std::string Engine::upload(const Model& m) {
             if (m.node_region[m.g(a, b)] != 6) continue;
             const int q = m.rnode_id[m.g(a, b)];
             if (q < 1 || q > R6.ngnode) continue;
-            if (b * m.dx > moho.z[n] + 0.5 * m.dx)
-              hv[n] = std::max(hv[n], R6.vel64[R6.slot_of_node[q - 1]]);
+            if (b * m.dx > moho.z[n] + 0.5 * m.dx) {
+              const int sq = R6.slot_of_node[q - 1];
+              if (R6.vel64[sq] > hv[n]) { hv[n] = R6.vel64[sq]; hvs[n] = sq; }
+            }
           }
       } else {
         hv[n] = R6.vel64[slot];
+        hvs[n] = slot;
       }
     }
     if (!(e = put(hw_slot_, hs, stream_)).empty()) return e;
     if (!(e = put(hw_v_, hv, stream_)).empty()) return e;
+    hw_slot_h_ = hs;
+    hw_vslot_h_ = hvs;
   }
   if (!(e = upload_trace_tables()).empty()) return e;
   npick_ = -1;
@@ -373,7 +378,8 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   if (max_slots >= (1ull << 30)) return "region too large for the eikonal solver (2^30 slots)";
   {
     // the lane's stream is idle here (the previous level ended with a sync)
-    const size_t per = sizeof(Fld64) + sizeof(Seed64) + 4 * sizeof(double) + 8 * sizeof(unsigned);
+    const size_t per = sizeof(Fld64) + sizeof(Seed64) + 4 * sizeof(double) + 8 * sizeof(unsigned) +
+                       sizeof(double*);
     std::string e0s = lane_reserve(L, (size_t)nf * per + kCtrN * 8 + 16 * 256);
     if (!e0s.empty()) return e0s;
   }
@@ -546,9 +552,19 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
   if (!hw.empty()) {
     if (!(e = put_lane(L, L.which, hw)).empty()) return e;
     L.hw.alloc(hw.size() * (size_t)m_.nx * sizeof(double));
+    // each field keeps its solved times at the sweep nodes (for the adjoint)
+    std::vector<double*> pre(hw.size());
+    for (size_t q = 0; q < hw.size(); ++q) {
+      FieldStore& S = fields_[items[hw[q]].first][items[hw[q]].second];
+      S.hwpre.alloc((size_t)m_.nx * sizeof(double));
+      if (!S.hwpre.p) return "device allocation failed (head-wave times)";
+      pre[q] = S.hwpre.as<double>();
+    }
+    if (!(e = put_lane(L, L.hwpre, pre)).empty()) return e;
     const double dx_if = m_.xpos[1] - m_.xpos[0];
     e64_headwave(dF, hw_slot_.as<int>(), hw_v_.as<double>(), dx_if, m_.nx,
-                 L.hw.as<double>(), L.which.as<int>(), (int)hw.size(), L.st);
+                 L.hw.as<double>(), L.which.as<int>(), (int)hw.size(), L.hwpre.as<double*>(),
+                 L.st);
     ++L.stats.launches;
     CK(cudaGetLastError());
   }

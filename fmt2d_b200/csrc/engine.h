@@ -58,6 +58,7 @@ struct DevRegionStore {
 // plus the solver state of the field.
 struct FieldStore {
   DevBuf T, G, Gout, fl, seed, clock;
+  DevBuf hwpre;   // PmP up: solved times at the head-wave sweep nodes (nx)
   bool solved = false;
 };
 
@@ -88,7 +89,7 @@ inline int chain_of(int tf) {
 struct SolveLane {
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
-  DevBuf fields, up, step, sx, sz, seeds, which, hw, ctr;
+  DevBuf fields, up, step, sx, sz, seeds, which, hw, hwpre, ctr;
   DevBuf sTn, sGn, sfln, spend, sclaim, slist, sover, sinq, scnt;
   SolveStats stats;
   bool not_converged = false;
@@ -99,7 +100,7 @@ struct SolveLane {
   char* pin = nullptr;
   size_t pin_cap = 0, pin_used = 0;
   void free_all() {
-    for (DevBuf* b : {&fields, &up, &step, &sx, &sz, &seeds, &which, &hw, &ctr, &sTn, &sGn, &sfln,
+    for (DevBuf* b : {&fields, &up, &step, &sx, &sz, &seeds, &which, &hw, &hwpre, &ctr, &sTn, &sGn, &sfln,
                       &spend, &sclaim, &slist, &sover, &sinq, &scnt})
       b->free_();
     if (pin) cudaFreeHost(pin);
@@ -129,6 +130,17 @@ class Engine {
   // per pick of the last trace: the ray's receiver end (seafloor entry point
   // of an in-water pick of phases 1-3, else the receiver) and the water time
   std::string trace_entries(double* water_time, double* entry_x, double* entry_z);
+  // Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks with
+  // t_obs >= 0 (phases 1-3) on the fields of the last forward (traced here:
+  // t_calc, valid), and its gradient w.r.t. the propagation-grid velocity
+  // (nx*nz, ix fastest; may be null) by the discrete adjoint of the fields.
+  // info (8 values, may be null): re-derived values that differ from the
+  // stored times, links outside their node's reader list, nodes the reverse
+  // sweep did not reach, its most rounds, fields, reached nodes, ms.
+  std::string misfit_gradient(const int* src, const int* phase, const double* rx,
+                              const double* rz, const double* t_obs, const double* sigma,
+                              int npick, double* misfit, double* t_calc, int* valid,
+                              double* grad_vel, double* info);
   double trace_ms() const { return trace_ms_; }
   long long frechet_nnz() const { return nnz_; }
   const Model& model() const { return m_; }
@@ -164,6 +176,7 @@ class Engine {
   DevBuf ifc_buf_[6][6];      // z, nx, nz, vel_top, vel_bot, izc
   Ifc64 ifc_[6];
   DevBuf hw_slot_, hw_v_;
+  std::vector<int> hw_slot_h_, hw_vslot_h_;   // host copies; the slot each hw_v value comes from
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
   DevBuf export_;             // region-order copy of a field being read back

@@ -579,4 +579,105 @@ int select_data(int npick, const int* phase, const double* obs, const double* t_
   return nd;
 }
 
+namespace {
+
+// The four propagation-grid nodes and bilinear weights of vel_side(m, px,
+// pzoff): vel_side's value is sum_k w[k] * m.vel[node[k]], summed in k order.
+void vel_side_w(const Model& m, double px, double pzoff, int* node, double* w) {
+  const int nx = m.nx, nz = m.nz;
+  const double dxv = m.xpos[1] - m.xpos[0];
+  int ivx = (int)std::floor((px - m.xpos[0]) / dxv);
+  ivx = std::max(0, std::min(nx - 2, ivx));
+  const double wx = std::min(1.0, std::max(0.0, (px - m.xpos[ivx]) / dxv));
+  int ivz;
+  double wz;
+  if (pzoff < grid_z(m, 0)) { ivz = 0; wz = 0.0; }
+  else if (pzoff >= grid_z(m, nz - 1)) { ivz = nz - 2; wz = 1.0; }
+  else {
+    for (ivz = 0; ivz < nz - 1; ++ivz)
+      if (pzoff >= grid_z(m, ivz) && pzoff < grid_z(m, ivz + 1)) break;
+    if (ivz >= nz - 1) ivz = nz - 2;
+    const double up = grid_z(m, ivz + 1) - grid_z(m, ivz);
+    wz = up > 0.0 ? (pzoff - grid_z(m, ivz)) / up : 0.0;
+  }
+  wz = std::min(1.0, std::max(0.0, wz));
+  node[0] = (int)m.g(ivx, ivz);
+  node[1] = (int)m.g(ivx + 1, ivz);
+  node[2] = (int)m.g(ivx, ivz + 1);
+  node[3] = (int)m.g(ivx + 1, ivz + 1);
+  w[0] = (1.0 - wx) * (1.0 - wz);
+  w[1] = wx * (1.0 - wz);
+  w[2] = (1.0 - wx) * wz;
+  w[3] = wx * wz;
+}
+
+}  // namespace
+
+std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
+                              std::vector<int>& slot, std::vector<double>& w) {
+  if (reg < 1 || reg > 6) return "region out of range";
+  const Region& r = m.reg[reg];
+  const int nx = m.nx;
+  const Interface& ft = m.ifc[r.itop];
+  const Interface& fb = m.ifc[r.ibot];
+  const double dx = m.dx;
+  const size_t nn = (size_t)nx * m.nz;
+  // per slot: up to four (node, weight) pairs, as finish_region assigns the
+  // slot's velocity
+  const size_t ns = r.nslots();
+  std::vector<int> sn(ns * 4, -1);
+  std::vector<double> sw(ns * 4, 0.0);
+  auto side_k = [&](int ix) {
+    int k = (int)std::lround((grid_x(m, ix) - m.xpos[0]) / m.dx);
+    return std::max(0, std::min(nx - 1, k));
+  };
+  for (int iz = r.z_lo; iz <= r.z_hi; ++iz)
+    for (int ix = 0; ix < nx; ++ix) {
+      if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
+      const size_t s = (size_t)r.slot_grid(ix, iz);
+      if (iz > 0 && !in_region(r, ix, iz - 1)) {
+        const int k = side_k(ix);
+        vel_side_w(m, m.xpos[k], ft.z[k] + dx, &sn[4 * s], &sw[4 * s]);
+      } else if (iz < m.nz - 1 && !in_region(r, ix, iz + 1)) {
+        const int k = side_k(ix);
+        vel_side_w(m, m.xpos[k], fb.z[k] - dx, &sn[4 * s], &sw[4 * s]);
+      } else {
+        sn[4 * s] = (int)m.g(ix, iz);
+        sw[4 * s] = 1.0;
+      }
+    }
+  for (int k = 0; k < nx; ++k) {
+    const size_t st = (size_t)r.slot_top(k), sb = (size_t)r.slot_bot(k);
+    vel_side_w(m, m.xpos[k], ft.z[k] + dx, &sn[4 * st], &sw[4 * st]);
+    vel_side_w(m, m.xpos[k], fb.z[k] - dx, &sn[4 * sb], &sw[4 * sb]);
+  }
+  // the map must reproduce every slot's velocity bit for bit
+  for (size_t s = 0; s < ns; ++s) {
+    if (sn[4 * s] < 0) continue;
+    double v = sw[4 * s] * m.vel[sn[4 * s]];
+    if (sw[4 * s] != 1.0 || sn[4 * s + 1] >= 0)
+      for (int k = 1; k < 4; ++k) v = v + sw[4 * s + k] * m.vel[sn[4 * s + k]];
+    if (v != r.vel64[s])
+      return "slot velocity map does not reproduce region " + std::to_string(reg) +
+             " slot " + std::to_string(s);
+  }
+  // transposed, node-major, slots ascending within a node
+  rp.assign(nn + 1, 0);
+  for (size_t s = 0; s < ns; ++s)
+    for (int k = 0; k < 4; ++k)
+      if (sn[4 * s + k] >= 0 && sw[4 * s + k] != 0.0) ++rp[sn[4 * s + k] + 1];
+  for (size_t i = 0; i < nn; ++i) rp[i + 1] += rp[i];
+  slot.assign(rp[nn], 0);
+  w.assign(rp[nn], 0.0);
+  std::vector<int> fill(rp.begin(), rp.end() - 1);
+  for (size_t s = 0; s < ns; ++s)
+    for (int k = 0; k < 4; ++k)
+      if (sn[4 * s + k] >= 0 && sw[4 * s + k] != 0.0) {
+        const int j = fill[sn[4 * s + k]]++;
+        slot[j] = (int)s;
+        w[j] = sw[4 * s + k];
+      }
+  return std::string();
+}
+
 }  // namespace fmt2d

@@ -106,6 +106,16 @@ void build_geometry(Model& m, const double* topo, const double* sed_z, const dou
 // (NULL keeps them); the geometry is rebuilt.  Returns an error message or "".
 std::string update_model(Model& m, const double* vel, const double* iface_z);
 
+// Region `reg`'s slot velocities as a linear map of the propagation-grid
+// velocity m.vel: interior grid slots take their node's value, slots next to
+// the region's interfaces and the interface slots take the bilinear samples
+// one grid step off the interface (vel_top / vel_bot).  Node-major CSR over
+// the nx*nz grid nodes (rp), entries (slot, weight) in ascending slot order.
+// Checks that the map reproduces every slot's velocity bit for bit; returns
+// an error message or "".
+std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
+                              std::vector<int>& slot, std::vector<double>& w);
+
 // Gaussian smoothing matrix of the smooth_type 2/3 LSQR layouts as 1-based
 // CSR over all n_inv_parms rows (rows it does not cover stay empty), mvscale
 // folded into the values: which 0 = R_h, 1 = R_v over the velocity

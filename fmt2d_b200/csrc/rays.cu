@@ -848,7 +848,76 @@ __global__ void k_sf_times(const TrModel* Mp, const SfJob* jobs, int njobs, int 
     J.out[i] = time_at(M, M.reg[J.reg], J.T, M.xpos[i], M.ifz[2][i]);
 }
 
+// The slots and weights through which time_at(px, pz) reads the field:
+// time_at = sum_k w[k] * T[s[k]] (k < the returned count), or 0 nodes where
+// it returns huge_time.
+__device__ int time_weights(const TrModel& M, const TrRegion& r, const double* T, double px,
+                            double pz, int* s, double* w) {
+  int ix = (int)floor((px - M.x0) / M.dx) + 1;
+  int iz = (int)floor((pz - 0.0) / M.dx) + 1;
+  ix = max(1, min(M.nx - 1, ix));
+  iz = max(1, min(M.nz - 1, iz));
+  const double w1 = clamp01((px - gxc(M, ix)) / M.dx);
+  const double w2 = clamp01((pz - gzc(M, iz)) / M.dx);
+  auto sn = [&](int a, int b) {
+    int q = region_node(M, r, a, b);
+    if (q < 0) q = nearby_node(M, r, a, b);
+    return q;
+  };
+  s[0] = sn(ix, iz);
+  s[1] = sn(ix + 1, iz);
+  s[2] = sn(ix, iz + 1);
+  s[3] = sn(ix + 1, iz + 1);
+  const double hh = kHugeT * 0.5;
+  bool all = true;
+  for (int k = 0; k < 4; ++k) all = all && s[k] >= 0 && T[s[k]] < hh;
+  if (all) {
+    w[0] = (1.0 - w1) * (1.0 - w2);
+    w[1] = w1 * (1.0 - w2);
+    w[2] = (1.0 - w1) * w2;
+    w[3] = w1 * w2;
+    return 4;
+  }
+  s[0] = nearest_node(M, r, px, pz);
+  if (s[0] < 0 || !(T[s[0]] < hh)) return 0;
+  w[0] = 1.0;
+  return 1;
+}
+
+// One thread per target field (src*13 + tf in tgt): every valid pick whose
+// phase ends in that field adds coef[p] times the weights of its
+// receiver-end time (at the entry point the trace recorded) to d.  Picks are
+// taken in order, so the sums do not depend on thread timing.
+__global__ void k_adj_picks(const TrModel* Mp, const TrField* fields, const TrPick* picks,
+                            const int* valid, const double* entry, const double* coef,
+                            int npick, const int* tgt, double* const* d, int ntgt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ntgt) return;
+  const TrModel& M = *Mp;
+  const int src = tgt[k] / 13, tf = tgt[k] % 13;
+  const double* T = fields[(size_t)src * 13 + tf].T;
+  const TrRegion& r = M.reg[c_tfreg[tf]];
+  double* dk = d[k];
+  for (int p = 0; p < npick; ++p) {
+    const TrPick pk = picks[p];
+    if (pk.src != src || !valid[p] || coef[p] == 0.0) continue;
+    if (c_tfs[pk.phase][c_ntf[pk.phase]] != tf) continue;
+    int sl[4];
+    double w[4];
+    const int n = time_weights(M, r, T, entry[3 * (size_t)p], entry[3 * (size_t)p + 1], sl, w);
+    for (int j = 0; j < n; ++j) dk[sl[j]] += coef[p] * w[j];
+  }
+}
+
 }  // namespace
+
+void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks, const int* valid,
+                  const double* entry, const double* coef, int npick, const int* tgt,
+                  double* const* d, int ntgt, cudaStream_t st) {
+  if (ntgt <= 0) return;
+  k_adj_picks<<<(ntgt + 63) / 64, 64, 0, st>>>(m, fields, picks, valid, entry, coef, npick, tgt,
+                                               d, ntgt);
+}
 
 void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStream_t st) {
   if (njobs <= 0) return;

@@ -64,4 +64,13 @@ void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, con
                const unsigned long long* off, unsigned long long* keys, double* vals,
                double* entry, cudaStream_t st);
 
+// Direct adjoint terms of the picks (the misfit's derivative with respect to
+// the node times of each pick's terminal field): for every valid pick of a
+// target field (tgt[k] = src*13 + tf), d[k][slot] += coef[pick] * w for the
+// nodes and bilinear weights through which its receiver-end time is read at
+// the entry point recorded by the trace (entry, 3 doubles per pick).
+void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks, const int* valid,
+                  const double* entry, const double* coef, int npick, const int* tgt,
+                  double* const* d, int ntgt, cudaStream_t st);
+
 }  // namespace fmt2d

@@ -241,6 +241,28 @@ FMT2D_API int fmt2d_stats(fmt2d_ctx* ctx, double* values, int n);
 FMT2D_API int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
                           const double* rz, int npick, double* t_calc, int* valid,
                           long long* nnz);
+
+/* Misfit and its gradient by the discrete adjoint of the time fields (no
+ * counterpart in the reference, whose inversion uses the ray-based Frechet
+ * rows G of fmt2d_trace; the gradient is the exact derivative of the
+ * reference's discrete forward, where G^T r is the ray-theory one).  On the
+ * fields of the last fmt2d_forward, for npick picks as in fmt2d_trace
+ * (phases 1-3) with observed times t_obs (< 0: no pick) and sigma > 0:
+ *   *misfit = 0.5 * sum over valid picks of ((t_calc - t_obs) / sigma)^2
+ * and, when grad_slow / grad_vel are not NULL, its derivative with respect to
+ * the propagation-grid slowness / velocity (nz*nx, ix fastest, the layout of
+ * fmt2d_model_velocity).  t_calc and valid are filled as fmt2d_trace fills
+ * them (the call traces the picks, so fmt2d_frechet_rows is available after
+ * it).  info (may be NULL) receives FMT2D_ADJ_N_INFO values: node values the
+ * adjoint could not re-derive, links outside their node's reader list, nodes
+ * its reverse sweep did not reach (all three 0 on success), the sweep's most
+ * rounds, fields, reached nodes, ms. */
+#define FMT2D_ADJ_N_INFO 8
+FMT2D_API int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* phase,
+                                    const double* rx, const double* rz, const double* t_obs,
+                                    const double* sigma, int npick, double* misfit,
+                                    double* t_calc, int* valid, double* grad_slow,
+                                    double* grad_vel, double* info);
 /* Per pick of the last fmt2d_trace (npick values each, any may be NULL): the
  * water leg's time (ray%water_time, 0 for a receiver below the seafloor or a
  * Pg_ss / Pg_ss2 pick) and the ray's receiver end (the seafloor entry point
