@@ -121,8 +121,8 @@ def lib():
     L.fmt2d_trace_entries.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fmt2d_misfit_gradient.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_int, P(C.c_double),
-                                        C.c_void_p,
-                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
     L.fmt2d_autotune.argtypes = [V, _dp, C.c_int, C.c_int, P(C.c_int), C.c_void_p]
     for name in header_symbols():
         getattr(L, name).restype = C.c_int

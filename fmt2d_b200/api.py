@@ -292,7 +292,8 @@ class Fmt2d:
         (phases 1-3; t_obs < 0: no pick) on the last forward's fields and its
         gradient by the discrete adjoint of the fields
         (fmt2d_misfit_gradient).  Returns a dict: misfit, t_calc, valid,
-        grad_slow and / or grad_vel ((nz, nx), as `want` asks), info (the
+        grad_slow and / or grad_vel ((nz, nx)) and / or grad_iface ((5, nx):
+        node depths of interfaces 1..5), as `want` asks, and info (the
         adjoint's counters, see the header)."""
         src = np.ascontiguousarray(src, dtype=np.int32)
         phase = np.ascontiguousarray(phase, dtype=np.int32)
@@ -306,10 +307,11 @@ class Fmt2d:
         J = C.c_double()
         gs = np.zeros(self.nx * self.nz) if "slow" in want else None
         gvel = np.zeros(self.nx * self.nz) if "vel" in want else None
+        gif = np.zeros(5 * self.nx) if "iface" in want else None
         info = np.zeros(8)
         self._check(self.L.fmt2d_misfit_gradient(
             self.h, N.ptr(src), N.ptr(phase), N.ptr(rx), N.ptr(rz), N.ptr(t_obs), N.ptr(sigma), n,
-            C.byref(J), N.ptr(t), N.ptr(v), N.ptr(gs), N.ptr(gvel), N.ptr(info)),
+            C.byref(J), N.ptr(t), N.ptr(v), N.ptr(gs), N.ptr(gvel), N.ptr(gif), N.ptr(info)),
             "fmt2d_misfit_gradient")
         self.npick, self.frechet_nnz = n, None
         out = {"misfit": J.value, "t_calc": t, "valid": v.astype(bool), "info": info}
@@ -317,6 +319,31 @@ class Fmt2d:
             out["grad_slow"] = gs.reshape(self.nz, self.nx)
         if gvel is not None:
             out["grad_vel"] = gvel.reshape(self.nz, self.nx)
+        if gif is not None:
+            out["grad_iface"] = gif.reshape(5, self.nx)
+        return out
+
+    def gradient_on_params(self, grad: dict, proj: dict | None = None) -> np.ndarray:
+        """A misfit_gradient result on the inversion parameters
+        (fmt2d_inv_index numbering: the velocity parameters, then the inverted
+        interface's nodes): d misfit / d slowness at each parameter's node and
+        d misfit / d depth at each interface node.  With proj (a projection()
+        dict), P^T times that vector: the gradient on the coarse grid's
+        parameters."""
+        inv, nvp, npar = self.inv_index()
+        g = np.zeros(npar)
+        act = inv > 0
+        g[inv[act] - 1] = grad["grad_slow"][act]
+        if npar > nvp:
+            if "grad_iface" not in grad:
+                raise ValueError("the gradient lacks grad_iface (want 'iface')")
+            g[nvp:] = grad["grad_iface"][self.iface_inv - 1][: npar - nvp]
+        if proj is None:
+            return g
+        rp, col, val = proj["P"]
+        rows = np.repeat(np.arange(npar), np.diff(rp))
+        out = np.zeros(proj["npar"])
+        np.add.at(out, col - 1, val * g[rows])
         return out
 
     def trace_entries(self):

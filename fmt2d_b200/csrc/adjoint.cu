@@ -112,6 +112,18 @@ __device__ inline Dn operator/(double a, const Dn& b) {
   for (int k = 0; k < kND; ++k) r.d[k] = f * b.d[k];
   return r;
 }
+__device__ inline Dn operator+(double a, const Dn& b) {
+  Dn r = b;
+  r.v = a + b.v;
+  return r;
+}
+__device__ inline Dn operator-(double a, const Dn& b) {
+  Dn r;
+  r.v = a - b.v;
+#pragma unroll
+  for (int k = 0; k < kND; ++k) r.d[k] = -b.d[k];
+  return r;
+}
 __device__ inline Dn operator-(const Dn& a, double b) {
   Dn r = a;
   r.v = a.v - b;
@@ -131,10 +143,10 @@ __device__ inline Dn dmax(const Dn& a, const Dn& b) { return b.v > a.v ? b : a; 
 // Where each dual input comes from: a same-field time (tslot), a slot
 // velocity (vslot) or the parent field's time (xslot).
 struct Inputs {
-  int tslot[kND], vslot[kND], xslot[kND];
+  int tslot[kND], vslot[kND], xslot[kND], zkey[kND];
   __device__ void clear() {
 #pragma unroll
-    for (int k = 0; k < kND; ++k) tslot[k] = vslot[k] = xslot[k] = -1;
+    for (int k = 0; k < kND; ++k) tslot[k] = vslot[k] = xslot[k] = zkey[k] = -1;
   }
 };
 
@@ -177,12 +189,15 @@ __device__ bool reg_dual(const DNb* p, const DNb* q, Dn& out) {
 }
 
 // time_from_1_node2d (ev::from_1): a copy when the member is within
-// 0.01*tolerance, else the member's time plus the straight ray.
-__device__ Dn from1_dual(const Mem& a, const Dn& aT, const Dn& av, double xu, double zu,
-                         const Dn& vu, double tol, bool& offered) {
-  const double dxu = xu - a.x, dzu = zu - a.z;
-  const double dist = sqrt(dxu * dxu + dzu * dzu);
-  if (dist < 0.01 * tol) {
+// 0.01*tolerance, else the member's time plus the straight ray.  Depths az
+// (the member) and zu (the node) are inputs: interface nodes move with their
+// interface.
+__device__ Dn from1_dual(const Mem& a, const Dn& aT, const Dn& av, const Dn& az, double xu,
+                         const Dn& zu, const Dn& vu, double tol, bool& offered) {
+  const double dxu = xu - a.x;
+  const Dn dzu = zu - az;
+  const Dn dist = dsqrt(dxu * dxu + dzu * dzu);
+  if (dist.v < 0.01 * tol) {
     offered = !a.copied;
     return aT;
   }
@@ -194,26 +209,29 @@ __device__ Dn from1_dual(const Mem& a, const Dn& aT, const Dn& av, double xu, do
 // time_from_2_nodes2d (ev::from_2): the first candidate it offers whose
 // value is `target` (the one the best-candidate rule kept).
 __device__ bool from2_dual(const Mem& n1, const Mem& n2, const Dn& T1, const Dn& T2,
-                           const Dn& v1, const Dn& v2, double xu, double zu, const Dn& vu,
-                           double tol, double target, Dn& out) {
-  const double r1x = n1.x - xu, r1z = n1.z - zu;
-  const double r2x = n2.x - xu, r2z = n2.z - zu;
-  if (sqrt(r1x * r1x + r1z * r1z) < 0.01 * tol) {
+                           const Dn& v1, const Dn& v2, const Dn& z1, const Dn& z2, double xu,
+                           const Dn& zu, const Dn& vu, double tol, double target, Dn& out) {
+  const double r1x = n1.x - xu;
+  const Dn r1z = z1 - zu;
+  const double r2x = n2.x - xu;
+  const Dn r2z = z2 - zu;
+  if (sqrt(r1x * r1x + r1z.v * r1z.v) < 0.01 * tol) {
     out = T1;
     return !n1.copied && out.v == target;
   }
-  if (sqrt(r2x * r2x + r2z * r2z) < 0.01 * tol) {
+  if (sqrt(r2x * r2x + r2z.v * r2z.v) < 0.01 * tol) {
     out = T2;
     return !n2.copied && out.v == target;
   }
-  const double ex = n2.x - n1.x, ez = n2.z - n1.z;
+  const double ex = n2.x - n1.x;
+  const double ez = z2.v - z1.v;
   if (sqrt(ex * ex + ez * ez) < 0.01 * tol) {
     bool offered = false;
-    out = from1_dual(n1, T1, v1, xu, zu, vu, tol, offered);
+    out = from1_dual(n1, T1, v1, z1, xu, zu, vu, tol, offered);
     return offered && out.v == target;
   }
   const Dn v12 = 0.5 * (v1 + v2);
-  const Dn dx_ = (n1.x - n2.x) / v12, dz_ = (n1.z - n2.z) / v12;
+  const Dn dx_ = (n1.x - n2.x) / v12, dz_ = (z1 - z2) / v12;
   const Dn dd = dx_ * dx_ + dz_ * dz_;
   const Dn px = (T1 - T2) / dd * dx_;
   const Dn pz = (T1 - T2) / dd * dz_;
@@ -225,16 +243,16 @@ __device__ bool from2_dual(const Mem& n1, const Mem& n2, const Dn& T1, const Dn&
   if (det.v < 0.0) return false;
   const Dn u1 = 0.5 * (-be + dsqrt(det)) / ae;
   const Dn u2 = 0.5 * (-be - dsqrt(det)) / ae;
-  double m1x = -r1z, m1z = r1x;
+  double m1x = -r1z.v, m1z = r1x;
   double l = sqrt(m1x * m1x + m1z * m1z);
   m1x /= l;
   m1z /= l;
-  if (m1x * r2x + m1z * r2z < 0.0) { m1x = -m1x; m1z = -m1z; }
-  double m2x = -r2z, m2z = r2x;
+  if (m1x * r2x + m1z * r2z.v < 0.0) { m1x = -m1x; m1z = -m1z; }
+  double m2x = -r2z.v, m2z = r2x;
   l = sqrt(m2x * m2x + m2z * m2z);
   m2x /= l;
   m2z /= l;
-  if (m2x * r1x + m2z * r1z < 0.0) { m2x = -m2x; m2z = -m2z; }
+  if (m2x * r1x + m2z * r1z.v < 0.0) { m2x = -m2x; m2z = -m2z; }
   for (int k = 0; k < 2; ++k) {
     const Dn& u = k == 0 ? u1 : u2;
     const Dn wx = px + u * qx, wz = pz + u * qz;
@@ -455,9 +473,12 @@ __device__ bool seed_dual(const AdjField& A, int s, int row, int col, Dn& val, I
       if (rr < D.r0[col] || rr > D.r1[col]) continue;
       if (rr != r) continue;
       const int ps = D.src_row * D.src_pitch + n;
-      const double xm = F.ifx[n], zm = D.ifc.z[n];
-      const double ddx = (F.x0 + col * h) - xm, ddz = r * h - zm;
-      const double dist = sqrt(ddx * ddx + ddz * ddz);
+      const double xm = F.ifx[n];
+      in.zkey[2] = A.seed_iface * 65536 + n;
+      const Dn zm = dvar(D.ifc.z[n], 2);
+      const double ddx = (F.x0 + col * h) - xm;
+      const Dn ddz = r * h - zm;
+      const Dn dist = dsqrt(ddx * ddx + ddz * ddz);
       const double v = FMT_RO(F.vel + s);
       in.xslot[0] = ps;
       const Dn Tn = dvar(D.src_T[ps], 0);
@@ -490,6 +511,11 @@ __device__ bool derive(const AdjField& A, int s, AdjLink& L) {
   L.xref = -1;
   L.xw = 0.0;
   L.kind = kAdjNone;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    L.z[j] = -1;
+    L.wz[j] = 0.0;
+  }
   const uint32_t code = FMT_RO(F.code + s);
   const double Ts = F.T[s];
   if (!(code & kInRegion) || !(Ts < kReachD)) return false;
@@ -588,12 +614,26 @@ __device__ bool derive(const AdjField& A, int s, AdjLink& L) {
     if (grid) cell_members_s(F, row, col, code, w.cell, m, ms);
     else iface_members_s(F, row - F.H, col, code, m, ms);
     const Mem& a = m[w.p];
+    // an interface node's depth is an input (interface id * 65536 + column)
+    auto zkey = [&](int slot) {
+      const int rr = slot / F.pitch;
+      if (rr < F.H) return -1;
+      return (rr == F.H ? A.itop : A.ibot) * 65536 + (slot - rr * F.pitch);
+    };
+    auto zin = [&](double z, int slot, int k) {
+      const int key = zkey(slot);
+      if (key < 0) return dconst(z);
+      in.zkey[k] = key;
+      return dvar(z, k);
+    };
+    const Dn zud = zin(zu, s, 7);
     if (w.kind == kAdjRay) {
       in.tslot[0] = ms[w.p];
       in.vslot[1] = ms[w.p];
       in.vslot[2] = s;
       bool offered = false;
-      val = from1_dual(a, dvar(a.T, 0), dvar(a.v, 1), xu, zu, dvar(vu, 2), F.tol, offered);
+      val = from1_dual(a, dvar(a.T, 0), dvar(a.v, 1), zin(a.z, ms[w.p], 3), xu, zud, dvar(vu, 2),
+                       F.tol, offered);
       ok = offered;
       const double dxu = xu - a.x, dzu = zu - a.z;
       kind = sqrt(dxu * dxu + dzu * dzu) < 0.01 * F.tol ? kAdjCopy : kAdjRay;
@@ -604,8 +644,9 @@ __device__ bool derive(const AdjField& A, int s, AdjLink& L) {
       in.vslot[2] = ms[w.p];
       in.vslot[3] = ms[w.q];
       in.vslot[4] = s;
-      ok = from2_dual(a, b, dvar(a.T, 0), dvar(b.T, 1), dvar(a.v, 2), dvar(b.v, 3), xu, zu,
-                      dvar(vu, 4), F.tol, best.t, val);
+      ok = from2_dual(a, b, dvar(a.T, 0), dvar(b.T, 1), dvar(a.v, 2), dvar(b.v, 3),
+                      zin(a.z, ms[w.p], 5), zin(b.z, ms[w.q], 6), xu, zud, dvar(vu, 4), F.tol,
+                      best.t, val);
       kind = kAdjPlane;
     }
   }
@@ -614,11 +655,12 @@ __device__ bool derive(const AdjField& A, int s, AdjLink& L) {
     return true;
   }
   L.kind = kind;
-  int nt = 0, nv = 0;
+  int nt = 0, nv = 0, nzr = 0;
   for (int k = 0; k < kND; ++k) {
     if (in.tslot[k] >= 0 && nt < 4) { L.t[nt] = in.tslot[k]; L.wt[nt++] = val.d[k]; }
     if (in.vslot[k] >= 0 && nv < 4) { L.v[nv] = in.vslot[k]; L.wv[nv++] = val.d[k]; }
     if (in.xslot[k] >= 0) { L.xref = in.xslot[k]; L.xw = val.d[k]; }
+    if (in.zkey[k] >= 0 && nzr < 3) { L.z[nzr] = in.zkey[k]; L.wz[nzr++] = val.d[k]; }
   }
   return true;
 }
@@ -846,6 +888,69 @@ __global__ void k_adj_swap_pre(AdjField* fs, const int* which, int nsel, const i
   p[n] = t;
 }
 
+// Depth gradient of field A's interface nodes in column c: the links that
+// read the depth of the region's top / bottom interface node (the node
+// itself and its spread targets; hand-off seeds excluded), the hand-off seeds
+// that read the parent interface's node (the child's seed band, columns
+// c-1..c+1), and the slots whose velocity is sampled off the interface.
+__global__ void k_adj_gz(AdjField* fs, int nf, int nx) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nx) return;
+  AdjField& A = fs[blockIdx.y];
+  const Fld64& F = A.F;
+  double g[3] = {0.0, 0.0, 0.0};
+  for (int side = 0; side < 2; ++side) {
+    const int S = (F.H + side) * F.pitch + c;
+    const int key = (side == 0 ? A.itop : A.ibot) * 65536 + c;
+    for (int q = -1; q < 16; ++q) {
+      const int k = q < 0 ? S : ev::spread_target_at(F, S, q);
+      if (k < 0) continue;
+      const AdjLink& L = A.link[k];
+      if (L.kind == kAdjHandOff) continue;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        if (L.z[r] == key) g[side] += L.wz[r] * A.lam[k];
+    }
+  }
+  if (A.level > 0) {
+    const int key = A.seed_iface * 65536 + c;
+    const int izf = A.seed.ifc.izc[c];
+    if (izf >= 0)
+      for (int cc = c - 1; cc <= c + 1; ++cc) {
+        if (cc < 0 || cc >= nx) continue;
+        for (int r = izf - 2; r <= izf + 3; ++r) {
+          const int br = r - F.z_lo;
+          if (br < 0 || br >= F.H) continue;
+          const int k = br * F.pitch + cc;
+          const AdjLink& L = A.link[k];
+          if (L.kind != kAdjHandOff) continue;
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            if (L.z[j] == key) g[2] += L.wz[j] * A.lam[k];
+        }
+      }
+  }
+  for (int e = A.zrp[c]; e < A.zrp[c + 1]; ++e) g[A.zside[e]] += A.gv[A.zslot[e]] * A.zdv[e];
+  A.gzf[c] = g[0];
+  A.gzf[nx + c] = g[1];
+  A.gzf[2 * (size_t)nx + c] = g[2];
+}
+
+// giface[(i - 1) * nx + c] += the fields' terms for interface i, fields in order.
+__global__ void k_adj_gz_sum(const AdjField* fs, int nf, int nx, double* giface) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y + 1;
+  if (c >= nx) return;
+  double g = giface[(size_t)(i - 1) * nx + c];
+  for (int k = 0; k < nf; ++k) {
+    const AdjField& A = fs[k];
+    if (A.itop == i) g += A.gzf[c];
+    if (A.ibot == i) g += A.gzf[nx + c];
+    if (A.level > 0 && A.seed_iface == i) g += A.gzf[2 * (size_t)nx + c];
+  }
+  giface[(size_t)(i - 1) * nx + c] = g;
+}
+
 __global__ void k_adj_grid(const AdjField* fs, int nf, const int* const* rp,
                            const int* const* slot, const double* const* w, size_t nnode,
                            double* gvel) {
@@ -893,6 +998,12 @@ void adj_swap_pre(AdjField* f, const int* which, int nsel, const int* hw_slot,
                   double* const* pre, int nx, cudaStream_t st) {
   if (nsel <= 0) return;
   k_adj_swap_pre<<<dim3((nx + 127) / 128, nsel), 128, 0, st>>>(f, which, nsel, hw_slot, pre, nx);
+}
+
+void adj_depth(AdjField* f, int nf, int nx, double* giface, cudaStream_t st) {
+  if (nf <= 0) return;
+  k_adj_gz<<<dim3((nx + 127) / 128, nf), 128, 0, st>>>(f, nf, nx);
+  k_adj_gz_sum<<<dim3((nx + 127) / 128, 5), 128, 0, st>>>(f, nf, nx, giface);
 }
 
 void adj_to_grid(const AdjField* f, int nf, const int* const* map_rp, const int* const* map_slot,
@@ -963,7 +1074,7 @@ constexpr int kTerminal[4] = {0, 1, 3, 5};   // phase -> terminal time field (ph
 std::string Engine::misfit_gradient(const int* src, const int* phase, const double* rx,
                                     const double* rz, const double* t_obs, const double* sigma,
                                     int npick, double* misfit, double* t_calc, int* valid,
-                                    double* grad_vel, double* info) {
+                                    double* grad_vel, double* grad_iface, double* info) {
   cudaSetDevice(device_);
   if (m_.nx == 0) return "no model uploaded";
   if (npick < 0) return "negative pick count";
@@ -998,24 +1109,31 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   }
   *misfit = J;
   const size_t nnode = (size_t)m_.nx * m_.nz;
-  DevBuf d_coef, d_gvel;
+  DevBuf d_coef, d_gvel, d_giface;
   if (!(e = adj_put(d_coef, coef, stream_)).empty()) return e;
   d_gvel.alloc(nnode * sizeof(double));
-  if (!d_gvel.p) return "device allocation failed (gradient)";
+  d_giface.alloc((size_t)5 * m_.nx * sizeof(double));
+  if (!d_gvel.p || !d_giface.p) return "device allocation failed (gradient)";
   ACK(cudaMemsetAsync(d_gvel.p, 0, nnode * sizeof(double), stream_));
-  // slot -> grid velocity maps of the regions in use
-  DevBuf map_rp[7], map_slot[7], map_w[7];
+  ACK(cudaMemsetAsync(d_giface.p, 0, (size_t)5 * m_.nx * sizeof(double), stream_));
+  // slot -> grid velocity maps of the regions in use, and their slots sampled
+  // off an interface (depth slopes)
+  DevBuf map_rp[7], map_slot[7], map_w[7], map_zrp[7], map_zslot[7], map_zside[7], map_zdv[7];
   for (int tf = 1; tf <= 5; ++tf) {
     bool used = false;
     for (int s = 0; s < ns; ++s) used = used || need[(size_t)s * 13 + tf];
     const int r = kTf[tf].reg;
     if (!used || map_rp[r].p) continue;
-    std::vector<int> rp, sl;
-    std::vector<double> w;
-    if (!(e = slot_velocity_map(m_, r, rp, sl, w)).empty()) return e;
+    std::vector<int> rp, sl, zrp, zsl, zsd;
+    std::vector<double> w, zdv;
+    if (!(e = slot_velocity_map(m_, r, rp, sl, w, &zrp, &zsl, &zsd, &zdv)).empty()) return e;
     if (!(e = adj_put(map_rp[r], rp, stream_)).empty()) return e;
     if (!(e = adj_put(map_slot[r], sl, stream_)).empty()) return e;
     if (!(e = adj_put(map_w[r], w, stream_)).empty()) return e;
+    if (!(e = adj_put(map_zrp[r], zrp, stream_)).empty()) return e;
+    if (!(e = adj_put(map_zslot[r], zsl, stream_)).empty()) return e;
+    if (!(e = adj_put(map_zside[r], zsd, stream_)).empty()) return e;
+    if (!(e = adj_put(map_zdv[r], zdv, stream_)).empty()) return e;
   }
   DevBuf d_hwvslot;
   if (!(e = adj_put(d_hwvslot, hw_vslot_h_, stream_)).empty()) return e;
@@ -1057,7 +1175,8 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     std::vector<size_t> off(nf + 1, 0);
     for (int i = 0; i < nf; ++i) off[i + 1] = off[i] + reg_[kTf[items[i].tf].reg].nslots;
     const size_t tot = off[nf];
-    DevBuf b_link, b_cnt, b_lam, b_d, b_gv, b_fa, b_fb, b_ctr;
+    DevBuf b_link, b_cnt, b_lam, b_d, b_gv, b_fa, b_fb, b_ctr, b_gz;
+    b_gz.alloc((size_t)nf * 3 * m_.nx * sizeof(double));
     b_link.alloc(tot * sizeof(AdjLink));
     b_cnt.alloc(tot * sizeof(unsigned));
     b_lam.alloc(tot * sizeof(double));
@@ -1066,7 +1185,8 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     b_fa.alloc(tot * sizeof(unsigned));
     b_fb.alloc(tot * sizeof(unsigned));
     b_ctr.alloc((size_t)nf * kAdjCtrN * sizeof(unsigned));
-    if (!b_link.p || !b_cnt.p || !b_lam.p || !b_d.p || !b_gv.p || !b_fa.p || !b_fb.p || !b_ctr.p)
+    if (!b_link.p || !b_cnt.p || !b_lam.p || !b_d.p || !b_gv.p || !b_fa.p || !b_fb.p || !b_ctr.p ||
+        !b_gz.p)
       return "device allocation failed (adjoint state)";
     ACK(cudaMemsetAsync(b_cnt.p, 0, tot * sizeof(unsigned), stream_));
     ACK(cudaMemsetAsync(b_lam.p, 0, tot * sizeof(double), stream_));
@@ -1088,6 +1208,14 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       A.fb = b_fb.as<unsigned>() + off[i];
       A.ctr = b_ctr.as<unsigned>() + (size_t)i * kAdjCtrN;
       A.level = I.level;
+      A.itop = m_.reg[I.reg].itop;
+      A.ibot = m_.reg[I.reg].ibot;
+      A.seed_iface = I.level > 0 ? I.istart : 0;
+      A.gzf = b_gz.as<double>() + (size_t)i * 3 * m_.nx;
+      A.zrp = map_zrp[I.reg].as<int>();
+      A.zslot = map_zslot[I.reg].as<int>();
+      A.zside = map_zside[I.reg].as<int>();
+      A.zdv = map_zdv[I.reg].as<double>();
       A.sx = src_x_[s];
       A.sz = src_z_[s];
       if (I.level == 0) {
@@ -1206,6 +1334,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     if (!(e = adj_put(d_mw, mw, stream_)).empty()) return e;
     adj_to_grid(dA, nf, d_mrp.as<const int* const>(), d_msl.as<const int* const>(),
                 d_mw.as<const double* const>(), nnode, d_gvel.as<double>(), stream_);
+    adj_depth(dA, nf, m_.nx, d_giface.as<double>(), stream_);
     ACK(cudaGetLastError());
     std::vector<unsigned> ctr((size_t)nf * kAdjCtrN);
     ACK(cudaMemcpyAsync(ctr.data(), b_ctr.p, ctr.size() * sizeof(unsigned),
@@ -1224,6 +1353,9 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   if (grad_vel)
     ACK(cudaMemcpyAsync(grad_vel, d_gvel.p, nnode * sizeof(double), cudaMemcpyDeviceToHost,
                         stream_));
+  if (grad_iface)
+    ACK(cudaMemcpyAsync(grad_iface, d_giface.p, (size_t)5 * m_.nx * sizeof(double),
+                        cudaMemcpyDeviceToHost, stream_));
   ACK(cudaStreamSynchronize(stream_));
   if (info) {
     info[0] = (double)cnt_bad;

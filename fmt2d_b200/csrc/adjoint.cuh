@@ -36,6 +36,8 @@ struct AdjLink {
   int xref;         // parent-field slot whose time a hand-off seed reads (-1: none)
   int kind;         // AdjKind
   double xw;        // its weight
+  int z[3];         // interface nodes whose depths it reads: interface id * 65536 + column
+  double wz[3];
 };
 
 // One field's adjoint state.
@@ -52,6 +54,15 @@ struct AdjField {
   double sx = 0, sz = 0;     // source position (level-0 fields)
   Seed64 seed;               // hand-off from the parent field (level > 0; seed.src_T set)
   int level = 0;
+  int itop = 0, ibot = 0;    // the region's top / bottom interface ids
+  int seed_iface = 0;        // the interface a hand-off seeds from (level > 0)
+  double* gzf = nullptr;     // 3*nx: depth gradient of the top, bottom and seed interfaces' nodes
+  // the region's slots whose velocity is sampled off an interface, by column
+  // (slot_velocity_map): slot, side, d velocity / d depth
+  const int* zrp = nullptr;
+  const int* zslot = nullptr;
+  const int* zside = nullptr;
+  const double* zdv = nullptr;
 };
 
 enum {
@@ -82,6 +93,10 @@ void adj_headwave(AdjField* f, const int* which, int nsel, const int* hw_slot,
 // Exchange the stored (swept) and the solved (pre) times at the sweep nodes.
 void adj_swap_pre(AdjField* f, const int* which, int nsel, const int* hw_slot,
                   double* const* pre, int nx, cudaStream_t st);
+// Interface-depth gradient per field (gzf: the region's top and bottom
+// interfaces and the hand-off interface, per column), then summed over the
+// fields in order into giface[(iface - 1) * nx + col] (interfaces 1..5).
+void adj_depth(AdjField* f, int nf, int nx, double* giface, cudaStream_t st);
 // gvel[node] += sum over fields k, in order, of sum over the region map
 // entries of the node of w * gv_k[slot] (map k: node-major CSR).
 void adj_to_grid(const AdjField* f, int nf, const int* const* map_rp, const int* const* map_slot,

@@ -349,7 +349,7 @@ int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, const double* 
 int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
                           const double* rz, const double* t_obs, const double* sigma, int npick,
                           double* misfit, double* t_calc, int* valid, double* grad_slow,
-                          double* grad_vel, double* info) {
+                          double* grad_vel, double* grad_iface, double* info) {
   if (!ctx || !misfit || npick < 0 ||
       (npick > 0 && (!src || !phase || !rx || !rz || !t_obs || !sigma || !t_calc || !valid)))
     return FMT2D_ERR_ARG;
@@ -362,7 +362,7 @@ int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* phase, cons
   std::vector<double> gv((grad_slow || grad_vel) ? nn : 0);
   const std::string e = ctx->eng->misfit_gradient(src, phase, rx, rz, t_obs, sigma, npick, misfit,
                                                   t_calc, valid, gv.empty() ? nullptr : gv.data(),
-                                                  info);
+                                                  grad_iface, info);
   if (!e.empty()) {
     const bool arg = e.find("range") != std::string::npos || e.find("phases") != std::string::npos ||
                      e.find("sigma") != std::string::npos;

@@ -133,14 +133,15 @@ class Engine {
   // Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks with
   // t_obs >= 0 (phases 1-3) on the fields of the last forward (traced here:
   // t_calc, valid), and its gradient w.r.t. the propagation-grid velocity
-  // (nx*nz, ix fastest; may be null) by the discrete adjoint of the fields.
+  // (nx*nz, ix fastest; may be null) and the interface node depths (5*nx,
+  // interfaces 1..5; may be null) by the discrete adjoint of the fields.
   // info (8 values, may be null): re-derived values that differ from the
   // stored times, links outside their node's reader list, nodes the reverse
   // sweep did not reach, its most rounds, fields, reached nodes, ms.
   std::string misfit_gradient(const int* src, const int* phase, const double* rx,
                               const double* rz, const double* t_obs, const double* sigma,
                               int npick, double* misfit, double* t_calc, int* valid,
-                              double* grad_vel, double* info);
+                              double* grad_vel, double* grad_iface, double* info);
   double trace_ms() const { return trace_ms_; }
   long long frechet_nnz() const { return nnz_; }
   const Model& model() const { return m_; }

@@ -611,10 +611,32 @@ void vel_side_w(const Model& m, double px, double pzoff, int* node, double* w) {
   w[3] = wx * wz;
 }
 
+// d vel_side(m, px, pzoff) / d pzoff: the bilinear sample's slope in depth
+// inside the bracketing rows (0 where the sample is clamped to the grid).
+double vel_side_dz(const Model& m, double px, double pzoff) {
+  const int nx = m.nx, nz = m.nz;
+  const double dxv = m.xpos[1] - m.xpos[0];
+  int ivx = (int)std::floor((px - m.xpos[0]) / dxv);
+  ivx = std::max(0, std::min(nx - 2, ivx));
+  const double wx = std::min(1.0, std::max(0.0, (px - m.xpos[ivx]) / dxv));
+  if (pzoff < grid_z(m, 0) || pzoff >= grid_z(m, nz - 1)) return 0.0;
+  int ivz;
+  for (ivz = 0; ivz < nz - 1; ++ivz)
+    if (pzoff >= grid_z(m, ivz) && pzoff < grid_z(m, ivz + 1)) break;
+  if (ivz >= nz - 1) return 0.0;
+  const double up = grid_z(m, ivz + 1) - grid_z(m, ivz);
+  if (!(up > 0.0)) return 0.0;
+  auto V = [&](int a, int b) { return m.vel[m.g(a, b)]; };
+  return ((1.0 - wx) * (V(ivx, ivz + 1) - V(ivx, ivz)) +
+          wx * (V(ivx + 1, ivz + 1) - V(ivx + 1, ivz))) / up;
+}
+
 }  // namespace
 
 std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
-                              std::vector<int>& slot, std::vector<double>& w) {
+                              std::vector<int>& slot, std::vector<double>& w,
+                              std::vector<int>* zrp, std::vector<int>* zslot,
+                              std::vector<int>* zside, std::vector<double>* zdv) {
   if (reg < 1 || reg > 6) return "region out of range";
   const Region& r = m.reg[reg];
   const int nx = m.nx;
@@ -631,6 +653,10 @@ std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
     int k = (int)std::lround((grid_x(m, ix) - m.xpos[0]) / m.dx);
     return std::max(0, std::min(nx - 1, k));
   };
+  // slots sampled off an interface: (column k, side 0 top / 1 bottom, slot,
+  // d velocity / d interface depth)
+  struct ZE { int k, side, s; double dv; };
+  std::vector<ZE> ze;
   for (int iz = r.z_lo; iz <= r.z_hi; ++iz)
     for (int ix = 0; ix < nx; ++ix) {
       if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
@@ -638,9 +664,11 @@ std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
       if (iz > 0 && !in_region(r, ix, iz - 1)) {
         const int k = side_k(ix);
         vel_side_w(m, m.xpos[k], ft.z[k] + dx, &sn[4 * s], &sw[4 * s]);
+        ze.push_back({k, 0, (int)s, vel_side_dz(m, m.xpos[k], ft.z[k] + dx)});
       } else if (iz < m.nz - 1 && !in_region(r, ix, iz + 1)) {
         const int k = side_k(ix);
         vel_side_w(m, m.xpos[k], fb.z[k] - dx, &sn[4 * s], &sw[4 * s]);
+        ze.push_back({k, 1, (int)s, vel_side_dz(m, m.xpos[k], fb.z[k] - dx)});
       } else {
         sn[4 * s] = (int)m.g(ix, iz);
         sw[4 * s] = 1.0;
@@ -650,6 +678,24 @@ std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
     const size_t st = (size_t)r.slot_top(k), sb = (size_t)r.slot_bot(k);
     vel_side_w(m, m.xpos[k], ft.z[k] + dx, &sn[4 * st], &sw[4 * st]);
     vel_side_w(m, m.xpos[k], fb.z[k] - dx, &sn[4 * sb], &sw[4 * sb]);
+    ze.push_back({k, 0, (int)st, vel_side_dz(m, m.xpos[k], ft.z[k] + dx)});
+    ze.push_back({k, 1, (int)sb, vel_side_dz(m, m.xpos[k], fb.z[k] - dx)});
+  }
+  if (zrp) {
+    std::stable_sort(ze.begin(), ze.end(), [](const ZE& a, const ZE& b) {
+      return a.k != b.k ? a.k < b.k : a.s < b.s;
+    });
+    zrp->assign(nx + 1, 0);
+    zslot->resize(ze.size());
+    zside->resize(ze.size());
+    zdv->resize(ze.size());
+    for (size_t i = 0; i < ze.size(); ++i) {
+      ++(*zrp)[ze[i].k + 1];
+      (*zslot)[i] = ze[i].s;
+      (*zside)[i] = ze[i].side;
+      (*zdv)[i] = ze[i].dv;
+    }
+    for (int k = 0; k < nx; ++k) (*zrp)[k + 1] += (*zrp)[k];
   }
   // the map must reproduce every slot's velocity bit for bit
   for (size_t s = 0; s < ns; ++s) {

@@ -112,9 +112,15 @@ std::string update_model(Model& m, const double* vel, const double* iface_z);
 // one grid step off the interface (vel_top / vel_bot).  Node-major CSR over
 // the nx*nz grid nodes (rp), entries (slot, weight) in ascending slot order.
 // Checks that the map reproduces every slot's velocity bit for bit; returns
-// an error message or "".
+// an error message or "".  With zrp set, also the slots whose velocity is a
+// sample off one of the region's interfaces, column-major CSR over the nx
+// interface nodes (zrp): slot, side (0 top, 1 bottom interface) and the
+// sample's derivative with respect to that interface node's depth.
 std::string slot_velocity_map(const Model& m, int reg, std::vector<int>& rp,
-                              std::vector<int>& slot, std::vector<double>& w);
+                              std::vector<int>& slot, std::vector<double>& w,
+                              std::vector<int>* zrp = nullptr, std::vector<int>* zslot = nullptr,
+                              std::vector<int>* zside = nullptr,
+                              std::vector<double>* zdv = nullptr);
 
 // Gaussian smoothing matrix of the smooth_type 2/3 LSQR layouts as 1-based
 // CSR over all n_inv_parms rows (rows it does not cover stay empty), mvscale

@@ -251,7 +251,11 @@ FMT2D_API int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, cons
  *   *misfit = 0.5 * sum over valid picks of ((t_calc - t_obs) / sigma)^2
  * and, when grad_slow / grad_vel are not NULL, its derivative with respect to
  * the propagation-grid slowness / velocity (nz*nx, ix fastest, the layout of
- * fmt2d_model_velocity).  t_calc and valid are filled as fmt2d_trace fills
+ * fmt2d_model_velocity); when grad_iface is not NULL, with respect to the
+ * node depths of interfaces 1..5 (5*nx, interface i's node ix at
+ * (i-1)*nx + ix; the depth moves the interface nodes of the cut cells, the
+ * velocities sampled off the interface and the stage hand-off distances,
+ * while region membership and cut cells are held).  t_calc and valid are filled as fmt2d_trace fills
  * them (the call traces the picks, so fmt2d_frechet_rows is available after
  * it).  info (may be NULL) receives FMT2D_ADJ_N_INFO values: node values the
  * adjoint could not re-derive, links outside their node's reader list, nodes
@@ -262,7 +266,7 @@ FMT2D_API int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* p
                                     const double* rx, const double* rz, const double* t_obs,
                                     const double* sigma, int npick, double* misfit,
                                     double* t_calc, int* valid, double* grad_slow,
-                                    double* grad_vel, double* info);
+                                    double* grad_vel, double* grad_iface, double* info);
 /* Per pick of the last fmt2d_trace (npick values each, any may be NULL): the
  * water leg's time (ray%water_time, 0 for a receiver below the seafloor or a
  * Pg_ss / Pg_ss2 pick) and the ray's receiver end (the seafloor entry point
