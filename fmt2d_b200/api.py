@@ -287,6 +287,22 @@ class Fmt2d:
         self.npick, self.frechet_nnz = n, nnz.value
         return t, v.astype(bool), nnz.value
 
+    def trace_times(self, src, phase, rx, rz):
+        """Receiver times and valid flags of picks on the last forward's fields,
+        without Frechet rows (fmt2d_trace_times).  Returns (t_calc, valid)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        phase = np.ascontiguousarray(phase, dtype=np.int32)
+        rx = np.ascontiguousarray(rx, dtype=np.float64)
+        rz = np.ascontiguousarray(rz, dtype=np.float64)
+        n = src.size
+        t = np.zeros(n)
+        v = np.zeros(n, np.int32)
+        self._check(self.L.fmt2d_trace_times(self.h, N.ptr(src), N.ptr(phase), N.ptr(rx),
+                                             N.ptr(rz), n, N.ptr(t), N.ptr(v)),
+                    "fmt2d_trace_times")
+        self.npick, self.frechet_nnz = n, None
+        return t, v.astype(bool)
+
     def misfit_gradient(self, src, phase, rx, rz, t_obs, sigma, want=("slow",)):
         """Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks
         (phases 1-3; t_obs < 0: no pick) on the last forward's fields and its

@@ -377,6 +377,21 @@ int fmt2d_misfit_gradient(fmt2d_ctx* ctx, const int* src, const int* phase, cons
   return FMT2D_OK;
 }
 
+int fmt2d_trace_times(fmt2d_ctx* ctx, const int* src, const int* phase, const double* rx,
+                      const double* rz, int npick, double* t_calc, int* valid) {
+  if (!ctx || npick < 0 || (npick > 0 && (!src || !phase || !rx || !rz || !t_calc || !valid)))
+    return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  if (!ctx->has_model) return ctx->fail(FMT2D_ERR_STATE, "no model uploaded");
+  if (ctx->eng->nsrc() == 0) return ctx->fail(FMT2D_ERR_STATE, "no forward solved");
+  const std::string e =
+      ctx->eng->trace(src, phase, rx, rz, npick, t_calc, valid, nullptr, /*rows=*/false);
+  if (!e.empty())
+    return ctx->fail(e.find("range") != std::string::npos ? FMT2D_ERR_ARG : FMT2D_ERR_CUDA, e);
+  return FMT2D_OK;
+}
+
 int fmt2d_frechet_rows(fmt2d_ctx* ctx, int* row_ptr, int* gindx, double* gval, int index_base) {
   if (!ctx || (index_base != 0 && index_base != 1)) return FMT2D_ERR_ARG;
   int code = 0;

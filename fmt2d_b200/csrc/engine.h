@@ -124,8 +124,9 @@ class Engine {
   // receiver x, z) on the fields of the last forward; the rows stay on the
   // device until frechet_rows copies them out (CSR over all picks, invalid
   // picks empty, columns 1-based parameter ids unless base 0).
+  // rows = false: receiver times and valid flags only (no Frechet rows).
   std::string trace(const int* src, const int* phase, const double* rx, const double* rz,
-                    int npick, double* t_calc, int* valid, long long* nnz);
+                    int npick, double* t_calc, int* valid, long long* nnz, bool rows = true);
   std::string frechet_rows(int* row_ptr, int* col, double* val, int base);
   // per pick of the last trace: the ray's receiver end (seafloor entry point
   // of an in-water pick of phases 1-3, else the receiver) and the water time

@@ -86,7 +86,7 @@ std::string Engine::upload_trace_tables() {
 }
 
 std::string Engine::trace(const int* src, const int* phase, const double* rx, const double* rz,
-                          int npick, double* t_calc, int* valid, long long* nnz) {
+                          int npick, double* t_calc, int* valid, long long* nnz, bool rows) {
   cudaSetDevice(device_);
   if (m_.nx == 0) return "no model uploaded";
   if (npick < 0) return "negative pick count";
@@ -161,7 +161,7 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
     }
   } ev;
   cudaEventRecord(ev.a, stream_);
-  rows_ = 0;
+  rows_ = rows ? 0 : -1;
   nnz_ = 0;
   npick_ = -1;   // no rows to hand out unless this trace completes
   if (npick > 0) {
@@ -173,6 +173,18 @@ std::string Engine::trace(const int* src, const int* phase, const double* rx, co
               nullptr, nullptr, nullptr, d_entry_.as<double>(), stream_);
     ++stats_.launches;
     TCK(cudaGetLastError());
+    if (!rows) {   // times only (the line search's compute_rms_after_forward)
+      TCK(cudaMemcpyAsync(t_calc, d_tcalc_.p, (size_t)npick * 8, cudaMemcpyDeviceToHost, stream_));
+      TCK(cudaMemcpyAsync(valid, d_valid_.p, (size_t)npick * 4, cudaMemcpyDeviceToHost, stream_));
+      cudaEventRecord(ev.b, stream_);
+      TCK(cudaStreamSynchronize(stream_));
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev.a, ev.b);
+      trace_ms_ = ms;
+      npick_ = npick;
+      if (nnz) *nnz = 0;
+      return std::string();
+    }
     // offsets of each pick's contributions (64-bit: long rays times many picks)
     unsigned long long* off = d_off_.as<unsigned long long>();
     size_t tmp_bytes = 0;
@@ -292,6 +304,7 @@ std::string Engine::trace_entries(double* water_time, double* entry_x, double* e
 std::string Engine::frechet_rows(int* row_ptr, int* col, double* val, int base) {
   cudaSetDevice(device_);
   if (npick_ < 0) return "no picks traced";
+  if (rows_ < 0) return "no picks traced with Frechet rows (the last trace computed times only)";
   if (row_ptr) {
     std::vector<int> rp(npick_ + 1, 0);
     if (npick_ > 0)

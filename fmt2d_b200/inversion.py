@@ -128,11 +128,15 @@ class Inversion:
             return 2 if self.iter % 4 == 0 else 1
         return self.p.alt_inv_mode
 
-    def forward_and_trace(self):
+    def forward_and_trace(self, rows: bool = True):
         """Forward of every source and the ray backtrace of every pick on the
-        current model; returns (t_calc, valid)."""
+        current model (with the Frechet rows, or times only for the line
+        search); returns (t_calc, valid)."""
         self.g.forward(self.src_x, self.p.phases)
-        t, valid, _ = self.g.trace(self.src, self.phase, self.rx, self.rz)
+        if rows:
+            t, valid, _ = self.g.trace(self.src, self.phase, self.rx, self.rz)
+        else:
+            t, valid = self.g.trace_times(self.src, self.phase, self.rx, self.rz)
         self.forwards += 1
         return t, valid
 
@@ -226,7 +230,7 @@ class Inversion:
         for k in range(self.ls_prev, len(LADDER)):
             s = LADDER[k]
             self.apply_step(vel0, z0, dm, s, s * p.iface_step_ratio)
-            rms_try = self.rms(*self.forward_and_trace())
+            rms_try = self.rms(*self.forward_and_trace(rows=False))
             if rms_try < rms_best:
                 rms_best, step_len, ok = rms_try, s, k
             if rms_try < rms_orig:

@@ -242,6 +242,13 @@ FMT2D_API int fmt2d_trace(fmt2d_ctx* ctx, const int* src, const int* phase, cons
                           const double* rz, int npick, double* t_calc, int* valid,
                           long long* nnz);
 
+/* fmt2d_trace without the Frechet rows: t_calc and valid only (the line
+ * search's compute_rms_after_forward, src/inversion2d.f90:3298-3339, needs no
+ * sensitivities).  fmt2d_frechet_rows then reports FMT2D_ERR_STATE. */
+FMT2D_API int fmt2d_trace_times(fmt2d_ctx* ctx, const int* src, const int* phase,
+                                const double* rx, const double* rz, int npick, double* t_calc,
+                                int* valid);
+
 /* Misfit and its gradient by the discrete adjoint of the time fields (no
  * counterpart in the reference, whose inversion uses the ray-based Frechet
  * rows G of fmt2d_trace; the gradient is the exact derivative of the

@@ -130,3 +130,23 @@ def test_trace_pg_401x121(oracle_lib):
         np.testing.assert_array_equal(idx, r["idx"])
         if idx.size:
             assert np.abs(val - r["val"]).max() <= 1e-4 * np.abs(r["val"]).max()
+
+
+def test_trace_times_only():
+    """fmt2d_trace_times (the line search's times-only trace) returns the
+    same receiver times and valid flags as fmt2d_trace, bit for bit, and
+    leaves no Frechet rows to read."""
+    from fmt2d_b200._native import Fmt2dError
+    from fmt2d_b200.api import Fmt2d
+    m = synth.small_model(phases=(1, 2, 3))
+    g = Fmt2d(0).upload(m)
+    g.forward(m.obs_x, (1, 2, 3))
+    P = m.picks
+    args = (P[:, 0].astype(np.int32), P[:, 1].astype(np.int32), P[:, 2].copy(), P[:, 3].copy())
+    t, v, _ = g.trace(*args)
+    t2, v2 = g.trace_times(*args)
+    assert np.array_equal(t.view(np.int64), t2.view(np.int64))
+    assert np.array_equal(v, v2)
+    with pytest.raises((Fmt2dError, RuntimeError)):
+        g.frechet_rows()
+    g.close()
