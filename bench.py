@@ -325,13 +325,19 @@ def timed_on(stream, fn):
     return out, a.elapsed_time(b)
 
 
-def rays_and_lsqr(g, m, stream):
+def rays_and_lsqr(g, m, stream, nsrc=None, phases=None):
     """Ray backtrace + Frechet rows of every pick of the model on the fields
     of the last forward (picks/s), then the damped, smoothed LSQR solve on the
     selected rows (s per LSQR iteration).  Observed times are the computed
-    ones plus seeded 40 ms Gaussian noise (config-1 pick noise)."""
+    ones plus seeded 40 ms Gaussian noise (config-1 pick noise).  nsrc /
+    phases: only the picks of the first nsrc sources and of those phases
+    (the fields a reduced run solved)."""
     from fmt2d_b200.api import select_data
     P = m.picks
+    if nsrc is not None:
+        P = P[P[:, 0] < nsrc]
+    if phases is not None:
+        P = P[np.isin(P[:, 1], phases)]
     src = P[:, 0].astype(np.int32)
     ph = P[:, 1].astype(np.int32)
     rx, rz = P[:, 2].copy(), P[:, 3].copy()
@@ -572,7 +578,7 @@ def run_ours(args, world, rank, local):
     # same steps, outside the timed region)
     try:
         g.forward(src, PHASES)
-        rays, lsqr, adjoint = rays_and_lsqr(g, m, stream)
+        rays, lsqr, adjoint = rays_and_lsqr(g, m, stream, src.size, PHASES)
     except Exception as ex:  # the eikonal line is the result; report why these are absent
         rays = lsqr = adjoint = {"unavailable": str(ex)[:200]}
 

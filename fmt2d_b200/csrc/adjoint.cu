@@ -708,25 +708,36 @@ __global__ void k_adj_front(AdjField* fs, int nf) {
   A.fa[atomicAdd(&A.ctr[kAdjCtrFront], 1u)] = (unsigned)s;
 }
 
-// lam[s] = d[s] + sum over the links that read s (found among its spread
-// targets, in their fixed order) of weight * lam[reader].
-__device__ double pull_lam(const AdjField& A, int s) {
-  double l = A.d[s];
-  for (int q = 0; q < 16; ++q) {
+// The readers of slot s (the links that read its time, found among its
+// spread targets in their fixed order) with their weights, written at
+// roff[s]: the order the sweep sums them in.
+__global__ void k_adj_readers(AdjField* fs, int nf, int* rk, double* rw) {
+  AdjField& A = fs[blockIdx.y];
+  const int ns = A.F.nslots();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns || A.rcnt[s] == 0u) return;
+  unsigned o = A.roff[s];
+  const unsigned end = o + A.rcnt[s];
+  for (int q = 0; q < 16 && o < end; ++q) {
     const int k = ev::spread_target_at(A.F, s, q);
     if (k < 0) continue;
     const AdjLink& K = A.link[k];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      if (K.t[j] == s) l += K.wt[j] * A.lam[k];
+      if (K.t[j] == s && o < end) {
+        rk[o] = k;
+        rw[o] = K.wt[j];
+        ++o;
+      }
   }
-  return l;
 }
 
 // Reverse sweep of one field per block: a node is processed once every link
 // reading it has been (its count reaches zero), so each node is listed once
-// and the loop ends after at most one round per node.
-__global__ void __launch_bounds__(1024) k_adj_sweep(AdjField* fs, int nf) {
+// and the loop ends after at most one round per node.  lam[s] = d[s] + the
+// sum over its readers, in list order, of weight * lam[reader].
+__global__ void __launch_bounds__(1024) k_adj_sweep(AdjField* fs, int nf, const int* rk,
+                                                    const double* rw) {
   AdjField& A = fs[blockIdx.x];
   __shared__ unsigned n_in, n_out;
   unsigned* fin = A.fa;
@@ -742,11 +753,14 @@ __global__ void __launch_bounds__(1024) k_adj_sweep(AdjField* fs, int nf) {
     if (n == 0) break;
     for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
       const int s = (int)fin[i];
-      A.lam[s] = pull_lam(A, s);
-      const AdjLink& S = A.link[s];
+      double l = A.d[s];
+      const unsigned o = A.roff[s], c = A.rcnt[s];
+      for (unsigned e = 0; e < c; ++e) l += rw[o + e] * A.lam[rk[o + e]];
+      A.lam[s] = l;
+      const int* ts = A.link[s].t;   // a link is 8-byte aligned: plain int loads
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int t = S.t[j];
+        const int t = ts[j];
         if (t < 0) continue;
         if (atomicSub(&A.cnt[t], 1u) == 1u) fout[atomicAdd(&n_out, 1u)] = (unsigned)t;
       }
@@ -972,11 +986,18 @@ void adj_links(AdjField* f, int nf, size_t max_slots, cudaStream_t st) {
   k_adj_links<<<grid, 256, 0, st>>>(f, nf);
 }
 
-void adj_sweep(AdjField* f, int nf, size_t max_slots, cudaStream_t st) {
+void adj_readers(AdjField* f, int nf, size_t max_slots, int* rk, double* rw, cudaStream_t st) {
+  if (nf <= 0) return;
+  const dim3 grid((unsigned)((max_slots + 255) / 256), nf);
+  k_adj_readers<<<grid, 256, 0, st>>>(f, nf, rk, rw);
+}
+
+void adj_sweep(AdjField* f, int nf, size_t max_slots, const int* rk, const double* rw,
+               cudaStream_t st) {
   if (nf <= 0) return;
   const dim3 grid((unsigned)((max_slots + 255) / 256), nf);
   k_adj_front<<<grid, 256, 0, st>>>(f, nf);
-  k_adj_sweep<<<nf, 1024, 0, st>>>(f, nf);
+  k_adj_sweep<<<nf, 1024, 0, st>>>(f, nf, rk, rw);
   k_adj_gv<<<grid, 256, 0, st>>>(f, nf);
 }
 
@@ -1018,6 +1039,7 @@ void adj_to_grid(const AdjField* f, int nf, const int* const* map_rp, const int*
 // ------------------------------------------------------------------ host
 #include "engine.h"
 #include "rays.cuh"
+#include <cub/cub.cuh>
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -1138,8 +1160,11 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   DevBuf d_hwvslot;
   if (!(e = adj_put(d_hwvslot, hw_vslot_h_, stream_)).empty()) return e;
   // sources in chunks that fit in device memory
+  // per slot: link, counts, adjoint, direct term, velocity gradient, work
+  // lists, reader count and offset, and up to 4 reader entries
   constexpr size_t kPerSlot = sizeof(AdjLink) + 2 * sizeof(unsigned) + 3 * sizeof(double) +
-                              2 * sizeof(unsigned);
+                              2 * sizeof(unsigned) + 2 * sizeof(unsigned) +
+                              4 * (sizeof(int) + sizeof(double));
   size_t free_b = 0, total_b = 0;
   ACK(cudaMemGetInfo(&free_b, &total_b));
   const size_t budget = free_b / 2;
@@ -1175,7 +1200,9 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     std::vector<size_t> off(nf + 1, 0);
     for (int i = 0; i < nf; ++i) off[i + 1] = off[i] + reg_[kTf[items[i].tf].reg].nslots;
     const size_t tot = off[nf];
-    DevBuf b_link, b_cnt, b_lam, b_d, b_gv, b_fa, b_fb, b_ctr, b_gz;
+    DevBuf b_link, b_cnt, b_lam, b_d, b_gv, b_fa, b_fb, b_ctr, b_gz, b_rcnt, b_roff;
+    b_rcnt.alloc(tot * sizeof(unsigned));
+    b_roff.alloc(tot * sizeof(unsigned));
     b_gz.alloc((size_t)nf * 3 * m_.nx * sizeof(double));
     b_link.alloc(tot * sizeof(AdjLink));
     b_cnt.alloc(tot * sizeof(unsigned));
@@ -1186,7 +1213,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     b_fb.alloc(tot * sizeof(unsigned));
     b_ctr.alloc((size_t)nf * kAdjCtrN * sizeof(unsigned));
     if (!b_link.p || !b_cnt.p || !b_lam.p || !b_d.p || !b_gv.p || !b_fa.p || !b_fb.p || !b_ctr.p ||
-        !b_gz.p)
+        !b_gz.p || !b_rcnt.p || !b_roff.p)
       return "device allocation failed (adjoint state)";
     ACK(cudaMemsetAsync(b_cnt.p, 0, tot * sizeof(unsigned), stream_));
     ACK(cudaMemsetAsync(b_lam.p, 0, tot * sizeof(double), stream_));
@@ -1212,6 +1239,8 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       A.ibot = m_.reg[I.reg].ibot;
       A.seed_iface = I.level > 0 ? I.istart : 0;
       A.gzf = b_gz.as<double>() + (size_t)i * 3 * m_.nx;
+      A.rcnt = b_rcnt.as<unsigned>() + off[i];
+      A.roff = b_roff.as<unsigned>() + off[i];
       A.zrp = map_zrp[I.reg].as<int>();
       A.zslot = map_zslot[I.reg].as<int>();
       A.zside = map_zside[I.reg].as<int>();
@@ -1268,20 +1297,27 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
         ACK(cudaGetLastError());
       }
       // the picks' terms on the terminal fields
-      std::vector<int> tgt;
+      // each target field's picks (valid, observed), in pick order
+      std::vector<int> tgt, tp(1, 0), tpk;
       std::vector<double*> dptr;
       for (int i = i0; i < i1; ++i)
         if (items[i].tf == 1 || items[i].tf == 3 || items[i].tf == 5) {
           tgt.push_back(items[i].s * 13 + items[i].tf);
           dptr.push_back(hf[i].d);
+          for (int p = 0; p < npick; ++p)
+            if (coef[p] != 0.0 && src[p] == items[i].s && kTerminal[phase[p]] == items[i].tf)
+              tpk.push_back(p);
+          tp.push_back((int)tpk.size());
         }
-      DevBuf d_tgt, d_dptr;
-      if (!tgt.empty() && npick > 0) {
+      DevBuf d_tgt, d_dptr, d_tp, d_tpk;
+      if (!tgt.empty() && !tpk.empty()) {
         if (!(e = adj_put(d_tgt, tgt, stream_)).empty()) return e;
         if (!(e = adj_put(d_dptr, dptr, stream_)).empty()) return e;
+        if (!(e = adj_put(d_tp, tp, stream_)).empty()) return e;
+        if (!(e = adj_put(d_tpk, tpk, stream_)).empty()) return e;
         tr_adj_picks(d_trmodel_.as<TrModel>(), d_trfields_.as<TrField>(), d_picks_.as<TrPick>(),
-                     d_valid_.as<int>(), d_entry_.as<double>(), d_coef.as<double>(), npick,
-                     d_tgt.as<int>(), d_dptr.as<double* const>(), (int)tgt.size(), stream_);
+                     d_entry_.as<double>(), d_coef.as<double>(), d_tgt.as<int>(), d_tp.as<int>(),
+                     d_tpk.as<int>(), d_dptr.as<double* const>(), (int)tgt.size(), stream_);
         ACK(cudaGetLastError());
       }
       // the head-wave sweep of the PmP up-going fields, reversed; their
@@ -1309,7 +1345,33 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
         ACK(cudaGetLastError());
       }
       adj_links(dA + i0, i1 - i0, max_slots, stream_);
-      adj_sweep(dA + i0, i1 - i0, max_slots, stream_);
+      ACK(cudaGetLastError());
+      // reader lists of the level: counts, offsets (relative to the level's
+      // first slot), then the lists
+      const size_t a0 = off[i0], n0 = off[i1] - off[i0];
+      unsigned* rc = b_rcnt.as<unsigned>() + a0;
+      unsigned* ro = b_roff.as<unsigned>() + a0;
+      ACK(cudaMemcpyAsync(rc, b_cnt.as<unsigned>() + a0, n0 * sizeof(unsigned),
+                          cudaMemcpyDeviceToDevice, stream_));
+      size_t scan_b = 0;
+      ACK(cub::DeviceScan::ExclusiveSum(nullptr, scan_b, rc, ro, (int)n0, stream_));
+      DevBuf scan_tmp;
+      scan_tmp.alloc(std::max<size_t>(scan_b, 16));
+      if (!scan_tmp.p) return "device allocation failed (reader scan)";
+      ACK(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_b, rc, ro, (int)n0, stream_));
+      unsigned last[2] = {0u, 0u};
+      ACK(cudaMemcpyAsync(&last[0], ro + n0 - 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                          stream_));
+      ACK(cudaMemcpyAsync(&last[1], rc + n0 - 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                          stream_));
+      ACK(cudaStreamSynchronize(stream_));
+      const size_t nref = (size_t)last[0] + last[1];
+      DevBuf b_rk, b_rw;
+      b_rk.alloc(std::max<size_t>(nref, 1) * sizeof(int));
+      b_rw.alloc(std::max<size_t>(nref, 1) * sizeof(double));
+      if (!b_rk.p || !b_rw.p) return "device allocation failed (reader lists)";
+      adj_readers(dA + i0, i1 - i0, max_slots, b_rk.as<int>(), b_rw.as<double>(), stream_);
+      adj_sweep(dA + i0, i1 - i0, max_slots, b_rk.as<int>(), b_rw.as<double>(), stream_);
       ACK(cudaGetLastError());
       if (!hw.empty()) {
         adj_swap_pre(dA, d_hw.as<int>(), (int)hw.size(), hw_slot_.as<int>(),

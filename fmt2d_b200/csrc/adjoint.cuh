@@ -63,6 +63,10 @@ struct AdjField {
   const int* zslot = nullptr;
   const int* zside = nullptr;
   const double* zdv = nullptr;
+  // each node's readers (links reading its time) as lists, built once per
+  // level: count and offset into the level's reader arrays
+  unsigned* rcnt = nullptr;
+  unsigned* roff = nullptr;
 };
 
 enum {
@@ -77,8 +81,13 @@ enum {
 
 // Links of every slot of every field; counts each slot's readers.
 void adj_links(AdjField* f, int nf, size_t max_slots, cudaStream_t st);
-// The reverse sweep (one block per field) and the velocity gradient per slot.
-void adj_sweep(AdjField* f, int nf, size_t max_slots, cudaStream_t st);
+// Each node's readers (reader slot, link weight) at roff, in the fixed order
+// the sweep sums them (spread targets in order, then link entries in order).
+void adj_readers(AdjField* f, int nf, size_t max_slots, int* rk, double* rw, cudaStream_t st);
+// The reverse sweep (one block per field) over the reader lists and the
+// velocity gradient per slot.
+void adj_sweep(AdjField* f, int nf, size_t max_slots, const int* rk, const double* rw,
+               cudaStream_t st);
 // Hand-off terms: child field c's adjoint at its hand-off seeds is added to
 // its parent's direct terms (pairs child[k] -> parent[k], parent interface row
 // src_row of the child's seed descriptor).

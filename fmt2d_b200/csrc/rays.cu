@@ -884,39 +884,54 @@ __device__ int time_weights(const TrModel& M, const TrRegion& r, const double* T
   return 1;
 }
 
-// One thread per target field (src*13 + tf in tgt): every valid pick whose
-// phase ends in that field adds coef[p] times the weights of its
-// receiver-end time (at the entry point the trace recorded) to d.  Picks are
-// taken in order, so the sums do not depend on thread timing.
-__global__ void k_adj_picks(const TrModel* Mp, const TrField* fields, const TrPick* picks,
-                            const int* valid, const double* entry, const double* coef,
-                            int npick, const int* tgt, double* const* d, int ntgt) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ntgt) return;
+// One block per target field (src*13 + tf in tgt), whose picks are
+// tpk[tp[k] .. tp[k+1]) in pick order: the threads find the weights of a
+// chunk of picks at once, then one thread adds coef[p] times them to d in
+// pick order, so the sums do not depend on thread timing.
+__global__ void __launch_bounds__(128) k_adj_picks(const TrModel* Mp, const TrField* fields,
+                                                   const TrPick* picks, const double* entry,
+                                                   const double* coef, const int* tgt,
+                                                   const int* tp, const int* tpk,
+                                                   double* const* d) {
+  const int k = blockIdx.x;
   const TrModel& M = *Mp;
   const int src = tgt[k] / 13, tf = tgt[k] % 13;
   const double* T = fields[(size_t)src * 13 + tf].T;
   const TrRegion& r = M.reg[c_tfreg[tf]];
   double* dk = d[k];
-  for (int p = 0; p < npick; ++p) {
-    const TrPick pk = picks[p];
-    if (pk.src != src || !valid[p] || coef[p] == 0.0) continue;
-    if (c_tfs[pk.phase][c_ntf[pk.phase]] != tf) continue;
-    int sl[4];
-    double w[4];
-    const int n = time_weights(M, r, T, entry[3 * (size_t)p], entry[3 * (size_t)p + 1], sl, w);
-    for (int j = 0; j < n; ++j) dk[sl[j]] += coef[p] * w[j];
+  __shared__ int s_n[128], s_sl[128][4];
+  __shared__ double s_w[128][4];
+  for (int base = tp[k]; base < tp[k + 1]; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    s_n[threadIdx.x] = 0;
+    if (i < tp[k + 1]) {
+      const int p = tpk[i];
+      int sl[4];
+      double w[4];
+      const int n = time_weights(M, r, T, entry[3 * (size_t)p], entry[3 * (size_t)p + 1], sl, w);
+      s_n[threadIdx.x] = n;
+      for (int j = 0; j < n; ++j) {
+        s_sl[threadIdx.x][j] = sl[j];
+        s_w[threadIdx.x][j] = coef[p] * w[j];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int m = min((int)blockDim.x, tp[k + 1] - base);
+      for (int t = 0; t < m; ++t)
+        for (int j = 0; j < s_n[t]; ++j) dk[s_sl[t][j]] += s_w[t][j];
+    }
+    __syncthreads();
   }
 }
 
 }  // namespace
 
-void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks, const int* valid,
-                  const double* entry, const double* coef, int npick, const int* tgt,
-                  double* const* d, int ntgt, cudaStream_t st) {
+void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks,
+                  const double* entry, const double* coef, const int* tgt, const int* tp,
+                  const int* tpk, double* const* d, int ntgt, cudaStream_t st) {
   if (ntgt <= 0) return;
-  k_adj_picks<<<(ntgt + 63) / 64, 64, 0, st>>>(m, fields, picks, valid, entry, coef, npick, tgt,
-                                               d, ntgt);
+  k_adj_picks<<<ntgt, 128, 0, st>>>(m, fields, picks, entry, coef, tgt, tp, tpk, d);
 }
 
 void tr_sf_times(const TrModel* m, const SfJob* jobs, int njobs, int nx, cudaStream_t st) {

@@ -65,12 +65,13 @@ void tr_launch(const TrModel* m, const TrField* fields, const double* src_x, con
                double* entry, cudaStream_t st);
 
 // Direct adjoint terms of the picks (the misfit's derivative with respect to
-// the node times of each pick's terminal field): for every valid pick of a
-// target field (tgt[k] = src*13 + tf), d[k][slot] += coef[pick] * w for the
-// nodes and bilinear weights through which its receiver-end time is read at
-// the entry point recorded by the trace (entry, 3 doubles per pick).
-void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks, const int* valid,
-                  const double* entry, const double* coef, int npick, const int* tgt,
-                  double* const* d, int ntgt, cudaStream_t st);
+// the node times of each pick's terminal field): for target field k
+// (tgt[k] = src*13 + tf) and each of its picks p = tpk[tp[k] .. tp[k+1]) in
+// order, d[k][slot] += coef[p] * w for the nodes and bilinear weights through
+// which its receiver-end time is read at the entry point recorded by the
+// trace (entry, 3 doubles per pick).
+void tr_adj_picks(const TrModel* m, const TrField* fields, const TrPick* picks,
+                  const double* entry, const double* coef, const int* tgt, const int* tp,
+                  const int* tpk, double* const* d, int ntgt, cudaStream_t st);
 
 }  // namespace fmt2d
