@@ -80,3 +80,22 @@ def ref_ops(o, G, nvp, mask, ws_v, ws_i, wd_v, wd_i):
         return np.where(keep, y, 0.0)
 
     return LinearOperator((nd + 2 * npar, npar), matvec=mv, rmatvec=rmv, dtype=np.float64), ws, wd
+
+
+def lsqr_problem(pyoracle, seed=5):
+    """A damped, smoothed LSQR problem on the small model for the partitioned
+    solver's tests: the oracle's rays give G (rows tagged with their source),
+    seeded residuals and dm_sum, gtg = the column sums of G^2."""
+    from fmt2d_b200 import synth
+    m = synth.small_model()
+    o = pyoracle.Oracle(m)
+    nd, npar, rp, gi, gv, _, used = oracle_G(o, m)
+    inv, nvp, _ = o.inv_idx()
+    rng = np.random.default_rng(seed)
+    G = csr_to_scipy(nd, npar, rp, gi, gv)
+    gtg = np.asarray(G.multiply(G).sum(axis=0)).ravel()
+    return dict(o=o, nd=nd, npar=npar, nvp=nvp, inv=inv, rp=rp, gi=gi, gv=gv,
+                src=used[:, 0].astype(int), res=rng.normal(0.0, 0.05, nd),
+                dm_sum=rng.normal(0.0, 1e-3, npar), gtg=gtg,
+                weights=dict(eps_min=1e-4 * float(gtg.max()), wdv=1.0, wdv_iface=0.5,
+                             w_smooth=10.0, w_smooth_iface=3.0))
