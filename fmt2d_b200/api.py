@@ -374,8 +374,8 @@ class Fmt2d:
     def frechet_rows(self, index_base: int = 1):
         """CSR (row_ptr, gindx, gval) of the last trace (fmt2d_frechet_rows)."""
         if self.frechet_nnz is None:
-            raise RuntimeError("Frechet rows: call trace() first (misfit_gradient traces the "
-                               "picks but does not report the row count)")
+            raise RuntimeError("Frechet rows: call trace() first (trace_times and "
+                               "misfit_gradient compute no rows)")
         rp = np.zeros(self.npick + 1, np.int32)
         gi = np.zeros(max(self.frechet_nnz, 1), np.int32)
         gv = np.zeros(max(self.frechet_nnz, 1))

@@ -1115,7 +1115,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   }
   const auto t0 = std::chrono::steady_clock::now();
   long long nnz = 0;
-  std::string e = trace(src, phase, rx, rz, npick, t_calc, valid, &nnz);
+  std::string e = trace(src, phase, rx, rz, npick, t_calc, valid, &nnz, /*rows=*/false);
   if (!e.empty()) return e;
   const int ns = nsrc();
   std::vector<double> coef(std::max(npick, 1), 0.0);
@@ -1139,23 +1139,24 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   ACK(cudaMemsetAsync(d_gvel.p, 0, nnode * sizeof(double), stream_));
   ACK(cudaMemsetAsync(d_giface.p, 0, (size_t)5 * m_.nx * sizeof(double), stream_));
   // slot -> grid velocity maps of the regions in use, and their slots sampled
-  // off an interface (depth slopes)
-  DevBuf map_rp[7], map_slot[7], map_w[7], map_zrp[7], map_zslot[7], map_zside[7], map_zdv[7];
+  // off an interface (depth slopes), built once per uploaded model
   for (int tf = 1; tf <= 5; ++tf) {
     bool used = false;
     for (int s = 0; s < ns; ++s) used = used || need[(size_t)s * 13 + tf];
     const int r = kTf[tf].reg;
-    if (!used || map_rp[r].p) continue;
+    if (!used || adj_map_version_[r] == model_version_) continue;
     std::vector<int> rp, sl, zrp, zsl, zsd;
     std::vector<double> w, zdv;
     if (!(e = slot_velocity_map(m_, r, rp, sl, w, &zrp, &zsl, &zsd, &zdv)).empty()) return e;
-    if (!(e = adj_put(map_rp[r], rp, stream_)).empty()) return e;
-    if (!(e = adj_put(map_slot[r], sl, stream_)).empty()) return e;
-    if (!(e = adj_put(map_w[r], w, stream_)).empty()) return e;
-    if (!(e = adj_put(map_zrp[r], zrp, stream_)).empty()) return e;
-    if (!(e = adj_put(map_zslot[r], zsl, stream_)).empty()) return e;
-    if (!(e = adj_put(map_zside[r], zsd, stream_)).empty()) return e;
-    if (!(e = adj_put(map_zdv[r], zdv, stream_)).empty()) return e;
+    DevBuf* M = adj_map_[r];
+    if (!(e = adj_put(M[0], rp, stream_)).empty()) return e;
+    if (!(e = adj_put(M[1], sl, stream_)).empty()) return e;
+    if (!(e = adj_put(M[2], w, stream_)).empty()) return e;
+    if (!(e = adj_put(M[3], zrp, stream_)).empty()) return e;
+    if (!(e = adj_put(M[4], zsl, stream_)).empty()) return e;
+    if (!(e = adj_put(M[5], zsd, stream_)).empty()) return e;
+    if (!(e = adj_put(M[6], zdv, stream_)).empty()) return e;
+    adj_map_version_[r] = model_version_;
   }
   DevBuf d_hwvslot;
   if (!(e = adj_put(d_hwvslot, hw_vslot_h_, stream_)).empty()) return e;
@@ -1241,10 +1242,10 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       A.gzf = b_gz.as<double>() + (size_t)i * 3 * m_.nx;
       A.rcnt = b_rcnt.as<unsigned>() + off[i];
       A.roff = b_roff.as<unsigned>() + off[i];
-      A.zrp = map_zrp[I.reg].as<int>();
-      A.zslot = map_zslot[I.reg].as<int>();
-      A.zside = map_zside[I.reg].as<int>();
-      A.zdv = map_zdv[I.reg].as<double>();
+      A.zrp = adj_map_[I.reg][3].as<int>();
+      A.zslot = adj_map_[I.reg][4].as<int>();
+      A.zside = adj_map_[I.reg][5].as<int>();
+      A.zdv = adj_map_[I.reg][6].as<double>();
       A.sx = src_x_[s];
       A.sz = src_z_[s];
       if (I.level == 0) {
@@ -1386,9 +1387,9 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     std::vector<const double*> mw(nf);
     for (int i = 0; i < nf; ++i) {
       const int r = kTf[items[i].tf].reg;
-      mrp[i] = map_rp[r].as<int>();
-      msl[i] = map_slot[r].as<int>();
-      mw[i] = map_w[r].as<double>();
+      mrp[i] = adj_map_[r][0].as<int>();
+      msl[i] = adj_map_[r][1].as<int>();
+      mw[i] = adj_map_[r][2].as<double>();
     }
     DevBuf d_mrp, d_msl, d_mw;
     if (!(e = adj_put(d_mrp, mrp, stream_)).empty()) return e;

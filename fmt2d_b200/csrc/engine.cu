@@ -237,6 +237,7 @@ std::string Engine::upload(const Model& m) {
   }
   if (!(e = upload_trace_tables()).empty()) return e;
   npick_ = -1;
+  ++model_version_;   // cached per-model tables (the adjoint's velocity maps) are stale
   CK(cudaStreamSynchronize(stream_));
   return std::string();
 }

@@ -179,6 +179,11 @@ class Engine {
   Ifc64 ifc_[6];
   DevBuf hw_slot_, hw_v_;
   std::vector<int> hw_slot_h_, hw_vslot_h_;   // host copies; the slot each hw_v value comes from
+  long long model_version_ = 0;               // bumped by every upload
+  // the adjoint's slot -> grid velocity maps per region (slot_velocity_map:
+  // rp, slot, w, zrp, zslot, zside, zdv) and the model version they belong to
+  DevBuf adj_map_[7][7];
+  long long adj_map_version_[7] = {-1, -1, -1, -1, -1, -1, -1};
   std::vector<std::array<FieldStore, 13>> fields_;
   std::vector<double> src_x_, src_z_;
   DevBuf export_;             // region-order copy of a field being read back

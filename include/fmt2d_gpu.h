@@ -262,9 +262,9 @@ FMT2D_API int fmt2d_trace_times(fmt2d_ctx* ctx, const int* src, const int* phase
  * node depths of interfaces 1..5 (5*nx, interface i's node ix at
  * (i-1)*nx + ix; the depth moves the interface nodes of the cut cells, the
  * velocities sampled off the interface and the stage hand-off distances,
- * while region membership and cut cells are held).  t_calc and valid are filled as fmt2d_trace fills
- * them (the call traces the picks, so fmt2d_frechet_rows is available after
- * it).  info (may be NULL) receives FMT2D_ADJ_N_INFO values: node values the
+ * while region membership and cut cells are held).  t_calc and valid are
+ * filled as fmt2d_trace fills them (the call traces the picks for their
+ * times, without Frechet rows).  info (may be NULL) receives FMT2D_ADJ_N_INFO values: node values the
  * adjoint could not re-derive, links outside their node's reader list, nodes
  * its reverse sweep did not reach (all three 0 on success), the sweep's most
  * rounds, fields, reached nodes, ms. */
