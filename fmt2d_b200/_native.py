@@ -99,6 +99,7 @@ def lib():
     L.fmt2d_trace.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                               C.c_void_p, C.c_void_p, P(C.c_longlong)]
     L.fmt2d_frechet_rows.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    L.fmt2d_set_iface_window.argtypes = [V, C.c_double]
     L.fmt2d_trace_times.argtypes = [V, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                     C.c_void_p, C.c_void_p]
     L.fmt2d_set_frechet.argtypes = [V, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,

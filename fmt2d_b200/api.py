@@ -483,6 +483,12 @@ class Fmt2d:
         self._check(self.L.fmt2d_lsqr_stats(self.h, C.byref(ms), C.byref(n)), "fmt2d_lsqr_stats")
         return {"ms": ms.value, "launches": n.value}
 
+    def set_iface_window(self, cells: float):
+        """Window of the stages seeded along an interface when set_schedule's
+        window_cells is 0 (fmt2d_set_iface_window; 0: none)."""
+        self._check(self.L.fmt2d_set_iface_window(self.h, float(cells)), "fmt2d_set_iface_window")
+        return self
+
     def set_schedule(self, window_cells: float = 0.0, max_passes: int = 6, max_steps: int = 0):
         """Eikonal solve schedule (fmt2d_set_schedule).  window_cells > 0 holds
         new times beyond a window of that many cells (at the region's largest

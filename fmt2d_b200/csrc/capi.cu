@@ -557,6 +557,14 @@ int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
   return FMT2D_OK;
 }
 
+int fmt2d_set_iface_window(fmt2d_ctx* ctx, double cells) {
+  if (!ctx || !(cells >= 0.0) || cells > 1.0e6) return FMT2D_ERR_ARG;
+  int code = 0;
+  if (!ctx->need_gpu(code)) return code;
+  ctx->eng->iface_window_cells = cells;
+  return FMT2D_OK;
+}
+
 int fmt2d_set_solve_threads(fmt2d_ctx* ctx, int threads) {
   if (!ctx) return FMT2D_ERR_ARG;
   int code = 0;

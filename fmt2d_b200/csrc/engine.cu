@@ -428,7 +428,7 @@ std::string Engine::solve_level(SolveLane& L, const std::vector<std::pair<int, i
     // the whole line at once; without a window far nodes take early times
     // that many later updates revise)
     const double wc = window_cells > 0.0 ? window_cells
-                      : (kTf[tf].level == 0 ? 0.0 : kIfaceWindowCells);
+                      : (kTf[tf].level == 0 ? 0.0 : iface_window_cells);
     wstep[i] = wc > 0.0 ? wc * m_.dx / D.vmax : kHugeD;
     if (tf == 5) hw.push_back(i);
   }

@@ -154,6 +154,8 @@ class Engine {
   // sources, kIfaceWindowCells for stages seeded along an interface
   double window_cells = 0.0;
   static constexpr double kIfaceWindowCells = 32.0;
+  // the default window of stages seeded along an interface (cells; 0: none)
+  double iface_window_cells = kIfaceWindowCells;
   static constexpr long long kDefaultMaxSteps = 4000000;
   long long max_steps = kDefaultMaxSteps;  // safety cap on the steps of one field's solve
   int max_passes = 6;             // solve passes (each followed by a check of every node)

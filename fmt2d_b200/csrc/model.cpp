@@ -2,6 +2,7 @@
 #include "model.h"
 #include <algorithm>
 #include <cmath>
+#include <thread>
 
 namespace fmt2d {
 
@@ -333,7 +334,14 @@ void build_geometry(Model& m, const double* topo, const double* sed_z, const dou
       f.vel_bot[i] = vel_side(m, m.xpos[i], f.z[i] + dx);
     }
   }
-  for (int k = 1; k <= 6; ++k) finish_region(m, m.reg[k]);
+  // each region's codes and velocities read the shared model and write only
+  // that region: one thread per region
+  {
+    std::vector<std::thread> th;
+    for (int k = 2; k <= 6; ++k) th.emplace_back([&m, k] { finish_region(m, m.reg[k]); });
+    finish_region(m, m.reg[1]);
+    for (auto& t : th) t.join();
+  }
   // inversion numbering: velocity nodes at or below the seafloor, iz outer
   // (frechet2d.f90:55-63, invert2d_main.f90:456-477)
   m.inv_idx.assign((size_t)nx * nz, 0);

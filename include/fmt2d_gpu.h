@@ -394,6 +394,11 @@ FMT2D_API int fmt2d_lsqr_stats(fmt2d_ctx* ctx, double* ms, int* launches);
  * takes more steps. */
 FMT2D_API int fmt2d_set_schedule(fmt2d_ctx* ctx, double window_cells, int max_passes,
                                  long long max_steps);
+/* The window of stages seeded along an interface when fmt2d_set_schedule's
+ * window_cells is 0 (default 32 cells at the region's largest velocity; 0: no
+ * window).  The results do not depend on it in the parity tests; the number
+ * of solver steps does. */
+FMT2D_API int fmt2d_set_iface_window(fmt2d_ctx* ctx, double cells);
 
 /* Threads of each field's solve block: 256, 384 or 512 (0: the default,
  * 384).  Results are the same bit for bit for every size (no evaluation of a

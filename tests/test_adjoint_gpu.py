@@ -1,5 +1,5 @@
 """Misfit gradient by the discrete adjoint of the time fields
-(fmt2d_misfit_gradient) on the small Pg / Pg+PmP model: observed times from
+(fmt2d_misfit_gradient) on the small Pg / Pg+PmP / PsedP model: observed times from
 the checkerboard model, gradient on the smooth model.
 
 * finite differences of the device forward + trace misfit on 32 seeded
@@ -47,8 +47,9 @@ def _observed(m, phases):
 
 
 def _case(phases):
-    true = synth.small_model()
-    start = synth.small_model(cb_amp=0.0)
+    kw = {"phases": (1, 2, 3)} if 2 in phases else {}
+    true = synth.small_model(**kw)
+    start = synth.small_model(cb_amp=0.0, **kw)
     obs = _observed(true, phases)
     P = start.picks
     keep = np.isin(P[:, 1], phases)
@@ -72,7 +73,7 @@ def _grad(g, picks, obs, want=("slow",)):
                              want=want)
 
 
-@pytest.mark.parametrize("phases", [(1,), (1, 3)])
+@pytest.mark.parametrize("phases", [(1,), (1, 3), (2,)])
 def test_gradient_matches_finite_differences(phases):
     """32 seeded nodes.  The discrete forward is a minimum over candidate
     updates, so the misfit is smooth only between the slowness values where a
