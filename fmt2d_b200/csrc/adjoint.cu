@@ -1345,6 +1345,24 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
                      d_pre.as<double* const>(), m_.nx, stream_);
         ACK(cudaGetLastError());
       }
+      // the swept times go back into the fields on every way out of this
+      // level (after its links and sweep, or on an error return)
+      struct SwapBack {
+        AdjField* f;
+        const int* which;
+        int n;
+        const int* slot;
+        double* const* pre;
+        int nx;
+        cudaStream_t st;
+        ~SwapBack() {
+          if (n > 0) {
+            adj_swap_pre(f, which, n, slot, pre, nx, st);
+            cudaStreamSynchronize(st);
+          }
+        }
+      } swap_back{dA, d_hw.as<int>(), (int)hw.size(), hw_slot_.as<int>(),
+                  d_pre.as<double* const>(), m_.nx, stream_};
       adj_links(dA + i0, i1 - i0, max_slots, stream_);
       ACK(cudaGetLastError());
       // reader lists of the level: counts, offsets (relative to the level's
@@ -1374,11 +1392,6 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       adj_readers(dA + i0, i1 - i0, max_slots, b_rk.as<int>(), b_rw.as<double>(), stream_);
       adj_sweep(dA + i0, i1 - i0, max_slots, b_rk.as<int>(), b_rw.as<double>(), stream_);
       ACK(cudaGetLastError());
-      if (!hw.empty()) {
-        adj_swap_pre(dA, d_hw.as<int>(), (int)hw.size(), hw_slot_.as<int>(),
-                     d_pre.as<double* const>(), m_.nx, stream_);
-        ACK(cudaGetLastError());
-      }
       ACK(cudaStreamSynchronize(stream_));
       i0 = i1;
     }
