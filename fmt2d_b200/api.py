@@ -305,7 +305,7 @@ class Fmt2d:
 
     def misfit_gradient(self, src, phase, rx, rz, t_obs, sigma, want=("slow",)):
         """Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks
-        (phases 1-3; t_obs < 0: no pick) on the last forward's fields and its
+        (phases 1-5; t_obs < 0: no pick) on the last forward's fields and its
         gradient by the discrete adjoint of the fields
         (fmt2d_misfit_gradient).  Returns a dict: misfit, t_calc, valid,
         grad_slow and / or grad_vel ((nz, nx)) and / or grad_iface ((5, nx):

@@ -29,7 +29,7 @@ class EikonalMisfit(torch.autograd.Function):
     picks, t_obs, sigma): slowness a (nz, nx) tensor on any device; iface_z
     None or an (nx,) tensor of the inverted interface's node depths; g an
     api.Fmt2d holding the model (its numbering must not change); picks a dict
-    of arrays src, phase, rx, rz (phases 1-3)."""
+    of arrays src, phase, rx, rz (phases 1-5)."""
 
     @staticmethod
     def forward(ctx, slowness, iface_z, g, src_x, phases, picks, t_obs, sigma):

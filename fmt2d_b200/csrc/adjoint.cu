@@ -1083,7 +1083,9 @@ std::string adj_put(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   return std::string();
 }
 
-constexpr int kTerminal[4] = {0, 1, 3, 5};   // phase -> terminal time field (phases 1-3)
+// phase -> terminal time field (Pg, PsedP, PmP, Pg_ss, Pg_ss2)
+constexpr int kTerminal[6] = {0, 1, 3, 5, 8, 12};
+inline bool terminal_tf(int tf) { return tf == 1 || tf == 3 || tf == 5 || tf == 8 || tf == 12; }
 
 }  // namespace
 
@@ -1101,8 +1103,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   if (m_.nx == 0) return "no model uploaded";
   if (npick < 0) return "negative pick count";
   for (int p = 0; p < npick; ++p) {
-    if (phase[p] < 1 || phase[p] > 3)
-      return "the adjoint covers phases 1-3 (Pg, PsedP, PmP)";
+    if (phase[p] < 1 || phase[p] > 5) return "pick phase out of range";
     if (!(sigma[p] > 0.0)) return "pick sigma must be positive";
   }
   {
@@ -1140,7 +1141,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
   ACK(cudaMemsetAsync(d_giface.p, 0, (size_t)5 * m_.nx * sizeof(double), stream_));
   // slot -> grid velocity maps of the regions in use, and their slots sampled
   // off an interface (depth slopes), built once per uploaded model
-  for (int tf = 1; tf <= 5; ++tf) {
+  for (int tf = 1; tf <= 12; ++tf) {
     bool used = false;
     for (int s = 0; s < ns; ++s) used = used || need[(size_t)s * 13 + tf];
     const int r = kTf[tf].reg;
@@ -1178,7 +1179,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     int s1 = s0;
     while (s1 < ns) {
       size_t b = 0;
-      for (int tf = 1; tf <= 5; ++tf)
+      for (int tf = 1; tf <= 12; ++tf)
         if (need[(size_t)s1 * 13 + tf]) b += reg_[kTf[tf].reg].nslots * kPerSlot;
       if (s1 > s0 && bytes + b > budget) break;
       bytes += b;
@@ -1188,7 +1189,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
     struct Item { int s, tf, level; };
     std::vector<Item> items;
     for (int s = s0; s < s1; ++s)
-      for (int tf = 1; tf <= 5; ++tf)
+      for (int tf = 1; tf <= 12; ++tf)
         if (need[(size_t)s * 13 + tf]) {
           if (!fields_[s][tf].solved) return "time field not solved (run the forward first)";
           items.push_back({s, tf, kTf[tf].level});
@@ -1302,7 +1303,7 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       std::vector<int> tgt, tp(1, 0), tpk;
       std::vector<double*> dptr;
       for (int i = i0; i < i1; ++i)
-        if (items[i].tf == 1 || items[i].tf == 3 || items[i].tf == 5) {
+        if (terminal_tf(items[i].tf)) {
           tgt.push_back(items[i].s * 13 + items[i].tf);
           dptr.push_back(hf[i].d);
           for (int p = 0; p < npick; ++p)

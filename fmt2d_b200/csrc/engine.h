@@ -132,7 +132,7 @@ class Engine {
   // of an in-water pick of phases 1-3, else the receiver) and the water time
   std::string trace_entries(double* water_time, double* entry_x, double* entry_z);
   // Misfit 0.5*sum(((t_calc - t_obs)/sigma)^2) over the valid picks with
-  // t_obs >= 0 (phases 1-3) on the fields of the last forward (traced here:
+  // t_obs >= 0 (phases 1-5) on the fields of the last forward (traced here:
   // t_calc, valid), and its gradient w.r.t. the propagation-grid velocity
   // (nx*nz, ix fastest; may be null) and the interface node depths (5*nx,
   // interfaces 1..5; may be null) by the discrete adjoint of the fields.

@@ -254,7 +254,7 @@ FMT2D_API int fmt2d_trace_times(fmt2d_ctx* ctx, const int* src, const int* phase
  * rows G of fmt2d_trace; the gradient is the exact derivative of the
  * reference's discrete forward, where G^T r is the ray-theory one).  On the
  * fields of the last fmt2d_forward, for npick picks as in fmt2d_trace
- * (phases 1-3) with observed times t_obs (< 0: no pick) and sigma > 0:
+ * (phases 1-5) with observed times t_obs (< 0: no pick) and sigma > 0:
  *   *misfit = 0.5 * sum over valid picks of ((t_calc - t_obs) / sigma)^2
  * and, when grad_slow / grad_vel are not NULL, its derivative with respect to
  * the propagation-grid slowness / velocity (nz*nx, ix fastest, the layout of

@@ -1,11 +1,13 @@
 """Misfit gradient by the discrete adjoint of the time fields
-(fmt2d_misfit_gradient) on the small Pg / Pg+PmP / PsedP model: observed times from
+(fmt2d_misfit_gradient) on the small model, per phase (Pg, Pg+PmP, PsedP,
+Pg_ss, Pg_ss2): observed times from
 the checkerboard model, gradient on the smooth model.
 
 * finite differences of the device forward + trace misfit on 32 seeded
   nodes agree with the adjoint within 1e-3 relative (central, step 1e-5
-  relative; between the one-sided slopes where the misfit is not
-  differentiable at the base model), and the central
+  relative, or 1e-6 where a winner changes inside the larger step; at a
+  point where the misfit is not differentiable, one of the one-sided slopes
+  or between them), and the central
   difference with the 1e-3 step agrees at most nodes;
 * the adjoint re-derives every node's stored time bit for bit, each link
   is found in its node's reader list and the reverse sweep reaches every node;
@@ -13,7 +15,8 @@ the checkerboard model, gradient on the smooth model.
 * the ray-based G^T r (Frechet rows of fmt2d_trace, the reference's
   sensitivity) agrees with it on coarse blocks;
 * the Moho-depth gradient agrees with finite differences in the node depths;
-* the torch.autograd.Function returns the same gradients."""
+* the torch.autograd.Function returns the same gradients; an unknown phase
+  is an error."""
 import numpy as np
 import pytest
 import torch
@@ -47,7 +50,11 @@ def _observed(m, phases):
 
 
 def _case(phases):
-    kw = {"phases": (1, 2, 3)} if 2 in phases else {}
+    kw = {}
+    if 2 in phases:
+        kw = {"phases": (1, 2, 3)}
+    elif set(phases) & {4, 5}:
+        kw = {"phases": (1, 4, 5)}
     true = synth.small_model(**kw)
     start = synth.small_model(cb_amp=0.0, **kw)
     obs = _observed(true, phases)
@@ -73,7 +80,7 @@ def _grad(g, picks, obs, want=("slow",)):
                              want=want)
 
 
-@pytest.mark.parametrize("phases", [(1,), (1, 3), (2,)])
+@pytest.mark.parametrize("phases", [(1,), (1, 3), (2,), (4,), (5,)])
 def test_gradient_matches_finite_differences(phases):
     """32 seeded nodes.  The discrete forward is a minimum over candidate
     updates, so the misfit is smooth only between the slowness values where a
@@ -111,16 +118,28 @@ def test_gradient_matches_finite_differences(phases):
         (jp, vp), (jm, vm) = J(j, h), J(j, -h)
         assert np.array_equal(vp, v_0) and np.array_equal(vm, v_0)
         c, f, b = (jp - jm) / (2 * h), (jp - j0) / h, (j0 - jm) / h
-        if rel(a, c) <= 1e-3:
-            central += 1
-        elif min(rel(a, f), rel(a, b)) <= 1e-3 or (
-                abs(f - b) > 1e-2 * abs(c) and
-                min(f, b) - 1e-3 * abs(c) <= a <= max(f, b) + 1e-3 * abs(c)):
+        def at_tie(c, f, b):
             # not differentiable at the base model: the adjoint follows the
             # forward's tie-breaks, one one-sided slope or between them
+            return min(rel(a, f), rel(a, b)) <= 1e-3 or (
+                abs(f - b) > 1e-2 * abs(c) and
+                min(f, b) - 1e-3 * abs(c) <= a <= max(f, b) + 1e-3 * abs(c))
+
+        if rel(a, c) <= 1e-3:
+            central += 1
+        elif at_tie(c, f, b):
             tie += 1
         else:
-            bad.append((int(j), float(a), float(c), float(f), float(b)))
+            # a change of winner inside the step: the same tests at 1e-6
+            h6 = 1e-6 * s0.flat[j]
+            jp6, jm6 = J(j, h6)[0], J(j, -h6)[0]
+            c6, f6, b6 = (jp6 - jm6) / (2 * h6), (jp6 - j0) / h6, (j0 - jm6) / h6
+            if rel(a, c6) <= 1e-3:
+                central += 1
+            elif at_tie(c6, f6, b6):
+                tie += 1
+            else:
+                bad.append((int(j), float(a), float(c), float(f), float(b), float(c6)))
         H = 1e-3 * s0.flat[j]
         coarse += rel(a, (J(j, H)[0] - J(j, -H)[0]) / (2 * H)) <= 1e-3
     g.close()
@@ -253,10 +272,10 @@ def test_autograd_function():
     g.close()
 
 
-def test_gradient_rejects_water_multiples():
+def test_gradient_rejects_unknown_phase():
     g, m, picks, obs = _case((1,))
     ph = picks["phase"].copy()
-    ph[0] = 4
+    ph[0] = 6
     with pytest.raises(Fmt2dError):
         g.misfit_gradient(picks["src"], ph, picks["rx"], picks["rz"], obs, SIGMA)
     g.close()
