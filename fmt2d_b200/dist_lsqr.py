@@ -48,41 +48,43 @@ def laplacian_csr(inv_idx: np.ndarray, nparm: int, iface_start: int, iface_nx: i
     neighbours, plus the 1-D interface Laplacian over parameters
     iface_start+1 .. iface_start+iface_nx (one-sided at the ends)."""
     import scipy.sparse as sp
-    nz, nx = inv_idx.shape
+    inv = np.asarray(inv_idx)
+    nz, nx = inv.shape
     rows, cols, vals = [], [], []
-    for iz in range(nz):
-        for ix in range(nx):
-            idx = int(inv_idx[iz, ix])
-            if idx <= 0:
-                continue
-            nb = 0
-            for jz, jx in ((iz, ix - 1), (iz, ix + 1), (iz - 1, ix), (iz + 1, ix)):
-                if 0 <= jz < nz and 0 <= jx < nx and inv_idx[jz, jx] > 0:
-                    rows.append(idx - 1)
-                    cols.append(int(inv_idx[jz, jx]) - 1)
-                    vals.append(1.0)
-                    nb += 1
-            rows.append(idx - 1)
-            cols.append(idx - 1)
-            vals.append(-float(nb))
+    nb = np.zeros((nz, nx))
+    # neighbour pairs along x and along z: +1 both ways, each counted once
+    for a, b in ((inv[:, :-1], inv[:, 1:]), (inv[:-1, :], inv[1:, :])):
+        both = (a > 0) & (b > 0)
+        i, j = a[both] - 1, b[both] - 1
+        rows += [i, j]
+        cols += [j, i]
+        vals += [np.ones(i.size), np.ones(i.size)]
+    act = inv > 0
+    nb[:, :-1] += act[:, 1:]
+    nb[:, 1:] += act[:, :-1]
+    nb[:-1, :] += act[1:, :]
+    nb[1:, :] += act[:-1, :]
+    d = inv[act] - 1
+    rows.append(d)
+    cols.append(d)
+    vals.append(-nb[act])
+    # the interface nodes: one-sided at the ends, centred inside
     st, nxi = iface_start, iface_nx
-    for ix in range(1, nxi + 1):
-        idx = st + ix
-        if idx < 1 or idx > nparm:
-            continue
-        if ix == 1:
-            if st + 2 <= nparm:
-                rows += [idx - 1, idx - 1]
-                cols += [st + 1, idx - 1]
-                vals += [1.0, -1.0]
-        elif ix == nxi:
-            rows += [idx - 1, idx - 1]
-            cols += [st + ix - 2, idx - 1]
-            vals += [1.0, -1.0]
-        else:
-            rows += [idx - 1, idx - 1, idx - 1]
-            cols += [st + ix - 2, st + ix, idx - 1]
-            vals += [1.0, 1.0, -2.0]
+    ix = np.arange(1, nxi + 1)
+    idx = st + ix
+    ok = (idx >= 1) & (idx <= nparm)
+    first, last, mid = ok & (ix == 1), ok & (ix == nxi) & (ix != 1), ok & (ix > 1) & (ix < nxi)
+    first &= st + 2 <= nparm
+    for sel, offs, w in ((first, (1,), -1.0), (last, (-1,), -1.0), (mid, (-1, 1), -2.0)):
+        r = idx[sel] - 1
+        for o in offs:
+            rows.append(r)
+            cols.append(r + o)
+            vals.append(np.ones(r.size))
+        rows.append(r)
+        cols.append(r)
+        vals.append(np.full(r.size, w))
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
     return sp.csr_matrix((vals, (rows, cols)), shape=(nparm, nparm))
 
 
