@@ -1131,6 +1131,10 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
       need[(size_t)src[p] * 13 + tf] = 1;
   }
   *misfit = J;
+  // the picks of each (source, terminal field), in pick order
+  std::vector<std::vector<int>> picks_of((size_t)std::max(ns, 1) * 13);
+  for (int p = 0; p < npick; ++p)
+    if (coef[p] != 0.0) picks_of[(size_t)src[p] * 13 + kTerminal[phase[p]]].push_back(p);
   const size_t nnode = (size_t)m_.nx * m_.nz;
   DevBuf d_coef, d_gvel, d_giface;
   if (!(e = adj_put(d_coef, coef, stream_)).empty()) return e;
@@ -1306,9 +1310,8 @@ std::string Engine::misfit_gradient(const int* src, const int* phase, const doub
         if (terminal_tf(items[i].tf)) {
           tgt.push_back(items[i].s * 13 + items[i].tf);
           dptr.push_back(hf[i].d);
-          for (int p = 0; p < npick; ++p)
-            if (coef[p] != 0.0 && src[p] == items[i].s && kTerminal[phase[p]] == items[i].tf)
-              tpk.push_back(p);
+          const std::vector<int>& pl = picks_of[(size_t)items[i].s * 13 + items[i].tf];
+          tpk.insert(tpk.end(), pl.begin(), pl.end());
           tp.push_back((int)tpk.size());
         }
       DevBuf d_tgt, d_dptr, d_tp, d_tpk;
