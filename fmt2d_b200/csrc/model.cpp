@@ -89,7 +89,9 @@ void build_interface(Model& m, int k, const double* zs) {
   }
 }
 
-void define_region(Model& m, Region& r, int itop, int ibot) {
+// A region's own tables (row range per column, node numbering, slots): they
+// read only the interfaces, so the six regions are built concurrently.
+void define_region(const Model& m, Region& r, int itop, int ibot) {
   r.itop = itop;
   r.ibot = ibot;
   const int nx = m.nx, nz = m.nz;
@@ -100,16 +102,18 @@ void define_region(Model& m, Region& r, int itop, int ibot) {
   for (int ix = 0; ix < nx; ++ix) {
     const double zt = iface_z_at(m, m.xpos, m.ifc[itop].z, grid_x(m, ix));
     const double zb = iface_z_at(m, m.xpos, m.ifc[ibot].z, grid_x(m, ix));
-    int a = -1, b = -2;
-    for (int iz = 0; iz < nz; ++iz) {
-      const double z = grid_z(m, iz);
-      if (zt <= z && z <= zb) {
-        if (a < 0) a = iz;
-        b = iz;
-      }
-    }
+    // the rows with zt <= z <= zb form one range (z = iz*dx grows with iz):
+    // start from the estimate and settle it with those same comparisons
+    int a = (int)std::ceil(zt / m.dx);
+    a = std::max(0, std::min(nz, a));
+    while (a > 0 && zt <= grid_z(m, a - 1)) --a;
+    while (a < nz && !(zt <= grid_z(m, a))) ++a;
+    int b = (int)std::floor(zb / m.dx);
+    b = std::max(-1, std::min(nz - 1, b));
+    while (b < nz - 1 && grid_z(m, b + 1) <= zb) ++b;
+    while (b >= 0 && !(grid_z(m, b) <= zb)) --b;
     r.col_base[ix] = ng;
-    if (a >= 0) {
+    if (a <= b) {
       r.r0[ix] = a;
       r.r1[ix] = b;
       ng += b - a + 1;
@@ -130,24 +134,35 @@ void define_region(Model& m, Region& r, int itop, int ibot) {
   r.tiles_y = (r.H + kTileH - 1) / kTileH;
   r.pitch = r.tiles_x * kTileW;
   r.slot_of_node.assign(r.nnode, 0);
-  // node ids run down each column (the reference's order); the grid tables
-  // are written row by row (row-major arrays)
+  // node ids run down each column (the reference's order), slots row by row
   for (int iz = zlo; iz <= zhi; ++iz)
     for (int ix = 0; ix < nx; ++ix) {
       if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
-      const size_t gi = m.g(ix, iz);
-      const int id = r.col_base[ix] + (iz - r.r0[ix]);
-      r.slot_of_node[id] = r.slot_grid(ix, iz);
-      m.node_region[gi] = r.id;
-      m.rnode_id[gi] = id + 1;
+      r.slot_of_node[r.col_base[ix] + (iz - r.r0[ix])] = r.slot_grid(ix, iz);
     }
-  m.rright[itop].assign(nx, 0);
-  m.rleft[ibot].assign(nx, 0);
   for (int k = 0; k < nx; ++k) {
     r.slot_of_node[ng + k] = r.slot_top(k);
     r.slot_of_node[ng + nx + k] = r.slot_bot(k);
-    m.rright[itop][k] = ng + k + 1;
-    m.rleft[ibot][k] = ng + nx + k + 1;
+  }
+}
+
+// The model-wide tables a region definition leaves (the last region that
+// claims a grid node owns it; the interface node id tables of its top and
+// bottom interface), applied in the reference's region order.
+void claim_region(Model& m, const Region& r) {
+  const int nx = m.nx;
+  for (int iz = r.z_lo; iz <= r.z_hi; ++iz)
+    for (int ix = 0; ix < nx; ++ix) {
+      if (iz < r.r0[ix] || iz > r.r1[ix]) continue;
+      const size_t gi = m.g(ix, iz);
+      m.node_region[gi] = r.id;
+      m.rnode_id[gi] = r.col_base[ix] + (iz - r.r0[ix]) + 1;
+    }
+  m.rright[r.itop].assign(nx, 0);
+  m.rleft[r.ibot].assign(nx, 0);
+  for (int k = 0; k < nx; ++k) {
+    m.rright[r.itop][k] = r.ngnode + k + 1;
+    m.rleft[r.ibot][k] = r.ngnode + nx + k + 1;
   }
 }
 
@@ -308,11 +323,20 @@ void build_geometry(Model& m, const double* topo, const double* sed_z, const dou
   m.node_region.assign((size_t)nx * nz, 0);
   m.rnode_id.assign((size_t)nx * nz, 0);
   for (int k = 1; k <= 6; ++k) m.reg[k] = Region(), m.reg[k].id = k;
-  for (int k = 1; k <= 4; ++k) define_region(m, m.reg[k], k, k + 1);
+  {
+    // top / bottom interface of regions 1..6
+    static const int kBounds[7][2] = {{0, 0}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {2, 5}, {2, 4}};
+    std::vector<std::thread> th;
+    for (int k = 2; k <= 6; ++k)
+      th.emplace_back([&m, k] { define_region(m, m.reg[k], kBounds[k][0], kBounds[k][1]); });
+    define_region(m, m.reg[1], kBounds[1][0], kBounds[1][1]);
+    for (auto& t : th) t.join();
+  }
+  for (int k = 1; k <= 4; ++k) claim_region(m, m.reg[k]);
   m.rright[2].clear();
   m.rleft[5].clear();
-  define_region(m, m.reg[5], 2, 5);
-  define_region(m, m.reg[6], 2, 4);
+  claim_region(m, m.reg[5]);
+  claim_region(m, m.reg[6]);
   // fully regular: inside some region, no cut cell among the four around it,
   // not on the grid border (propagate2d.f90:1941-1979)
   m.fully_regular.assign((size_t)nx * nz, 0);
